@@ -1,0 +1,221 @@
+"""ctypes binding of the C ABI in ``include/drift_b200.h`` (``libdrift_b200.so``).
+
+This is the boundary a foreign-language host binds; the
+parity tests, the smoke check and the benchmark call the kernels through it.
+Functions here raise ``RuntimeError`` with the library's message when a call
+fails; nothing falls back to a CPU implementation.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdrift_b200.so"
+
+DOPR54, DOP853 = 0, 1
+POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN = 0, 1, 2, 3
+EXACT, FMA = 0, 1
+PLAIN, PERSISTENT = 0, 1
+INITIAL_STEP_SENTINEL = -9999.99
+PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT = range(5)
+
+# Every symbol the header declares.
+EXPORTED = (
+    "drift_abi_version",
+    "drift_result_string",
+    "drift_last_error",
+    "drift_host_alloc",
+    "drift_host_free",
+    "drift_potential_bovy",
+    "drift_query_workspace",
+    "drift_integrate",
+    "drift_integrate_host",
+    "drift_galpy_dopr54",
+    "drift_galpy_dop853",
+)
+
+
+class DriftPotential(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("amp", ctypes.c_double),
+        ("b", ctypes.c_double),
+        ("mn_amp", ctypes.c_double),
+        ("mn_a", ctypes.c_double),
+        ("mn_b", ctypes.c_double),
+        ("nfw_amp", ctypes.c_double),
+        ("nfw_a", ctypes.c_double),
+        ("bulge_alpha", ctypes.c_double),
+        ("bulge_rc", ctypes.c_double),
+        ("bulge_k", ctypes.c_double),
+        ("bulge_gamma_s", ctypes.c_double),
+    ]
+
+
+class DriftLaunch(ctypes.Structure):
+    _fields_ = [
+        ("method", ctypes.c_int32),
+        ("precision", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("block_size", ctypes.c_int32),
+        ("potential", DriftPotential),
+        ("n", ctypes.c_int64),
+        ("y0", ctypes.c_void_p),
+        ("nt", ctypes.c_int64),
+        ("ts", ctypes.c_void_p),
+        ("t0", ctypes.c_double),
+        ("t_end", ctypes.c_void_p),
+        ("out", ctypes.c_void_p),
+        ("y_final", ctypes.c_void_p),
+        ("rtol_ln", ctypes.c_double),
+        ("atol_ln", ctypes.c_double),
+        ("dt_one", ctypes.c_double),
+        ("max_steps", ctypes.c_int64),
+        ("timeout_s", ctypes.c_double),
+        ("status", ctypes.c_void_p),
+        ("err_code", ctypes.c_void_p),
+        ("n_accepted", ctypes.c_void_p),
+        ("n_rejected", ctypes.c_void_p),
+        ("workspace", ctypes.c_void_p),
+        ("workspace_bytes", ctypes.c_size_t),
+    ]
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libdrift_b200.so (raises if it is not built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise RuntimeError(f"{LIB_PATH} is not built; run __graft_entry__.build()")
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.drift_abi_version.restype = ctypes.c_int
+        L.drift_result_string.restype = ctypes.c_char_p
+        L.drift_result_string.argtypes = [ctypes.c_int]
+        L.drift_last_error.restype = ctypes.c_char_p
+        L.drift_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]
+        L.drift_host_free.argtypes = [ctypes.c_void_p]
+        L.drift_potential_bovy.argtypes = [ctypes.POINTER(DriftPotential)] + [ctypes.c_double] * 8
+        L.drift_query_workspace.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.POINTER(ctypes.c_size_t)]
+        L.drift_integrate.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
+        L.drift_integrate_host.argtypes = [ctypes.POINTER(DriftLaunch)]
+        L.drift_galpy_dopr54.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 3 + [ctypes.c_void_p]
+        L.drift_galpy_dop853.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 2 + [ctypes.c_void_p]
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = "drift call") -> None:
+    if rc != 0:
+        L = lib()
+        raise RuntimeError(f"{what} failed: {L.drift_result_string(rc).decode()} "
+                           f"({L.drift_last_error().decode()})")
+
+
+# Reference constants of the Bovy composite (shared/src/potential.rs:103-112)
+# and the cutoff power-law bulge (alpha = 1.8, rc = 1.9/8, F_r(1) = -0.05).
+BOVY_DEFAULTS = dict(alpha=1.8, rc=1.9 / 8.0, bulge_force=0.05, mn_amp=0.7574802019,
+                     mn_a=3.0 / 8.0, mn_b=0.28 / 8.0, nfw_amp=4.852230533528, nfw_a=16.0 / 8.0)
+
+
+def kepler(amp: float = 1.0) -> DriftPotential:
+    return DriftPotential(kind=POT_KEPLER, amp=amp)
+
+
+def kepler_cartesian(amp: float = 1.0) -> DriftPotential:
+    return DriftPotential(kind=POT_KEPLER_CARTESIAN, amp=amp)
+
+
+def plummer(amp: float = 1.0, b: float = 1.0) -> DriftPotential:
+    return DriftPotential(kind=POT_PLUMMER, amp=amp, b=b)
+
+
+def bovy(**overrides) -> DriftPotential:
+    p = dict(BOVY_DEFAULTS)
+    p.update(overrides)
+    pot = DriftPotential()
+    check(lib().drift_potential_bovy(ctypes.byref(pot), p["alpha"], p["rc"], p["bulge_force"],
+                                     p["mn_amp"], p["mn_a"], p["mn_b"], p["nfw_amp"], p["nfw_a"]),
+          "drift_potential_bovy")
+    return pot
+
+
+def _ptr(a) -> int | None:
+    return None if a is None else a.ctypes.data
+
+
+def make_launch(method: int, pot: DriftPotential, n: int, nt: int, *, rtol: float, atol: float,
+                precision: int = EXACT, schedule: int = PERSISTENT, block_size: int = 0,
+                dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
+                timeout_s: float = 0.0, t0: float = 0.0) -> DriftLaunch:
+    L = DriftLaunch()
+    L.method, L.precision, L.schedule, L.block_size = method, precision, schedule, block_size
+    L.potential = pot
+    L.n, L.nt, L.t0 = n, nt, t0
+    # LogTolerance::from_linear: the reference hands its kernels ln(tolerance).
+    L.rtol_ln, L.atol_ln = math.log(rtol), math.log(atol)
+    L.dt_one, L.max_steps, L.timeout_s = dt_one, max_steps, timeout_s
+    return L
+
+
+def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None, nt=None,
+                   t0: float = 0.0, rtol: float = 1e-12, atol: float = 1e-12,
+                   precision: int = EXACT, schedule: int = PERSISTENT, block_size: int = 0,
+                   dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
+                   timeout_s: float = 0.0, want_out: bool = True, out=None) -> dict:
+    """drift_integrate_host: host arrays in, host arrays out."""
+    y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
+    n = y0.shape[0]
+    if ts is not None:
+        ts = np.ascontiguousarray(ts, dtype=np.float64)
+        nt = len(ts)
+    else:
+        t_end = np.ascontiguousarray(t_end, dtype=np.float64)
+        assert nt is not None and t_end.shape == (n,)
+    L = make_launch(method, pot, n, nt, rtol=rtol, atol=atol, precision=precision,
+                    schedule=schedule, block_size=block_size, dt_one=dt_one,
+                    max_steps=max_steps, timeout_s=timeout_s, t0=t0)
+    if want_out and out is None:
+        out = np.empty((nt, n, 6))
+    res = dict(
+        out=out if want_out else None,
+        y_final=np.empty((n, 6)),
+        status=np.empty(n, np.uint8),
+        err=np.empty(n, np.int32),
+        accepted=np.empty(n, np.uint32),
+        rejected=np.empty(n, np.uint32),
+    )
+    L.y0 = _ptr(y0)
+    L.ts = _ptr(ts)
+    L.t_end = _ptr(t_end)
+    L.out = _ptr(res["out"])
+    L.y_final = _ptr(res["y_final"])
+    L.status = _ptr(res["status"])
+    L.err_code = _ptr(res["err"])
+    L.n_accepted = _ptr(res["accepted"])
+    L.n_rejected = _ptr(res["rejected"])
+    check(lib().drift_integrate_host(ctypes.byref(L)), "drift_integrate_host")
+    return res
+
+
+def query_workspace(L: DriftLaunch) -> int:
+    b = ctypes.c_size_t(0)
+    check(lib().drift_query_workspace(ctypes.byref(L), ctypes.byref(b)), "drift_query_workspace")
+    return b.value
+
+
+def integrate_device(L: DriftLaunch, stream: int = 0) -> None:
+    """drift_integrate on device pointers already stored in ``L``."""
+    check(lib().drift_integrate(ctypes.byref(L), ctypes.c_void_p(stream)), "drift_integrate")
+
+
+def exported_symbols() -> dict[str, bool]:
+    L = lib()
+    return {name: hasattr(L, name) for name in EXPORTED}

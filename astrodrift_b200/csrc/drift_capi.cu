@@ -1,0 +1,523 @@
+// drift_capi.cu -- the C ABI declared in include/drift_b200.h.
+//
+// Host-side validation, launch geometry, a library-owned persistent device
+// context (stream and grow-only buffers per device) and the host-buffer path
+// that pipelines particle chunks: copy-in, integration and copy-out of
+// different chunks overlap on two streams.  In the reference every stage
+// creates a CUDA context, JIT-loads the module and copies a zeroed output
+// buffer to the device (src/dispatch/gpu/cuda_oxide.rs:9-86); none of that is
+// repeated here.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "drift_b200.h"
+#include "drift_launch_args.cuh"
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg)
+{
+    g_last_error = msg;
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? DRIFT_ERROR_OUT_OF_MEMORY : DRIFT_ERROR_CUDA;
+}
+
+#define DRIFT_CUDA_TRY(expr, what)                 \
+    do {                                           \
+        cudaError_t e_ = (expr);                   \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+constexpr int64_t DEFAULT_MAX_STEPS = 100000000;  // 10^8 attempts per particle
+constexpr int DEFAULT_BLOCK = 128;
+constexpr size_t CURSOR_BYTES = 256;  // one 8-byte cursor, padded to an allocation granule
+
+// Device buffer that only grows.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need)
+    {
+        if (need <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMalloc(&ptr, need);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+    template <class T>
+    T *as() const
+    {
+        return static_cast<T *>(ptr);
+    }
+};
+
+struct HostBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need)
+    {
+        if (need <= bytes) return cudaSuccess;
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        cudaError_t e = cudaMallocHost(&ptr, need);
+        if (e == cudaSuccess) bytes = need;
+        return e;
+    }
+};
+
+// Library-owned state of one device: created on first use, kept for the
+// life of the process.
+struct DeviceContext {
+    int device = -1;
+    int sm_count = 0;
+    std::mutex mu;  // serialises host-buffer calls that share the buffers below
+    cudaStream_t streams[2] = {nullptr, nullptr};
+    cudaEvent_t done[2] = {nullptr, nullptr};
+    DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor;
+    HostBuf stage[2];
+};
+
+std::mutex g_ctx_mu;
+std::vector<DeviceContext *> g_ctx;
+
+int current_context(DeviceContext **out)
+{
+    int dev = -1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail(DRIFT_ERROR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lock(g_ctx_mu);
+    if ((int)g_ctx.size() <= dev) g_ctx.resize(dev + 1, nullptr);
+    if (!g_ctx[dev]) {
+        auto *c = new DeviceContext();
+        c->device = dev;
+        DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev),
+                       "cudaDeviceGetAttribute");
+        for (int i = 0; i < 2; i++) {
+            DRIFT_CUDA_TRY(cudaStreamCreateWithFlags(&c->streams[i], cudaStreamNonBlocking),
+                           "cudaStreamCreate");
+            DRIFT_CUDA_TRY(cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming),
+                           "cudaEventCreate");
+        }
+        g_ctx[dev] = c;
+    }
+    *out = g_ctx[dev];
+    return DRIFT_SUCCESS;
+}
+
+bool is_finite_value(double v) { return std::isfinite(v); }
+
+int validate(const drift_launch *L, bool device_pointers)
+{
+    if (!L) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "launch is NULL");
+    if (L->method != DRIFT_DOPR54 && L->method != DRIFT_DOP853)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown method");
+    if (L->precision != DRIFT_PRECISION_EXACT && L->precision != DRIFT_PRECISION_FMA)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown precision");
+    if (L->schedule != DRIFT_SCHEDULE_PLAIN && L->schedule != DRIFT_SCHEDULE_PERSISTENT)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown schedule");
+    if (L->block_size != 0 && (L->block_size < 32 || L->block_size > 128 || L->block_size % 32))
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "block_size must be 0 or a multiple of 32 in [32, 128]");
+    const int k = L->potential.kind;
+    if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown potential kind");
+    if (L->n < 1) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "n must be >= 1");
+    if (L->n > (int64_t(1) << 40)) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "n is too large");
+    if (L->nt < 2 || L->nt > INT32_MAX - 1)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "nt must be in [2, 2^31 - 2]");
+    if (!L->y0) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0 is NULL");
+    if (!L->ts && !L->t_end) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "either ts or t_end is required");
+    if (!L->ts && !is_finite_value(L->t0)) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "t0 must be finite");
+    if (!is_finite_value(L->rtol_ln) || !is_finite_value(L->atol_ln))
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "tolerances must be finite logarithms");
+    if (device_pointers &&
+        (reinterpret_cast<uintptr_t>(L->y0) % 16 || (L->out && reinterpret_cast<uintptr_t>(L->out) % 16) ||
+         (L->y_final && reinterpret_cast<uintptr_t>(L->y_final) % 16)))
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0, out and y_final must be 16-byte aligned");
+    return DRIFT_SUCCESS;
+}
+
+int block_of(const drift_launch *L) { return L->block_size ? L->block_size : DEFAULT_BLOCK; }
+
+drift::KernelArgs make_args(const drift_launch *L)
+{
+    drift::KernelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = L->n;
+    a.y0 = L->y0;
+    a.nt = (int32_t)L->nt;
+    a.persistent = L->schedule == DRIFT_SCHEDULE_PERSISTENT;
+    a.ts = L->ts;
+    a.t0 = L->t0;
+    a.t_end = L->t_end;
+    a.out = L->out;
+    a.y_final = L->y_final;
+    // The reference's DOP853 exponentiates the logarithmic tolerances at the
+    // start of every particle (dop853.rs:340-341); the same host libm exp is
+    // applied once here.
+    a.rtol = std::exp(L->rtol_ln);
+    a.atol = std::exp(L->atol_ln);
+    a.tol54.e_rtol = a.rtol;
+    a.tol54.e_atol = a.atol;
+    a.dt_one = L->dt_one;
+    a.max_steps = L->max_steps > 0 ? L->max_steps : DEFAULT_MAX_STEPS;
+    a.timeout_ns = L->timeout_s > 0 ? (uint64_t)(L->timeout_s * 1e9) : 0;
+    a.status = L->status;
+    a.err_code = L->err_code;
+    a.n_accepted = L->n_accepted;
+    a.n_rejected = L->n_rejected;
+    a.potential = L->potential;
+    return a;
+}
+
+cudaError_t launch_args(const drift::KernelArgs &a, int method, int precision, int grid, int block,
+                        cudaStream_t s)
+{
+    return precision == DRIFT_PRECISION_EXACT ? drift::launch_exact(a, method, grid, block, s)
+                                              : drift::launch_fma(a, method, grid, block, s);
+}
+
+int grid_of(DeviceContext *ctx, const drift_launch *L, int64_t n, int block, int *grid)
+{
+    int64_t blocks = (n + block - 1) / block;
+    if (L->schedule == DRIFT_SCHEDULE_PERSISTENT) {
+        int per_sm = 0;
+        cudaError_t e = L->precision == DRIFT_PRECISION_EXACT
+                            ? drift::occupancy_exact(L->method, L->potential.kind, block, &per_sm)
+                            : drift::occupancy_fma(L->method, L->potential.kind, block, &per_sm);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        int64_t cap = (int64_t)std::max(per_sm, 1) * ctx->sm_count;
+        blocks = std::min(blocks, cap);
+    }
+    if (blocks > INT32_MAX) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "too many particles for one launch");
+    *grid = (int)blocks;
+    return DRIFT_SUCCESS;
+}
+
+// Launch on device buffers.  `cursor` is needed by the persistent schedule.
+int launch_device(DeviceContext *ctx, const drift_launch *L, void *cursor, cudaStream_t s)
+{
+    drift::KernelArgs a = make_args(L);
+    const int block = block_of(L);
+    int grid = 0;
+    int rc = grid_of(ctx, L, L->n, block, &grid);
+    if (rc) return rc;
+    if (a.persistent) {
+        a.cursor = static_cast<unsigned long long *>(cursor);
+        DRIFT_CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s), "cudaMemsetAsync");
+    }
+    DRIFT_CUDA_TRY(launch_args(a, L->method, L->precision, grid, block, s), "kernel launch");
+    return DRIFT_SUCCESS;
+}
+
+bool is_pinned(const void *p)
+{
+    cudaPointerAttributes attr;
+    if (cudaPointerGetAttributes(&attr, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return attr.type == cudaMemoryTypeHost;
+}
+
+}  // namespace
+
+extern "C" {
+
+int drift_abi_version(void) { return DRIFT_ABI_VERSION; }
+
+const char *drift_result_string(int code)
+{
+    switch (code) {
+    case DRIFT_SUCCESS: return "success";
+    case DRIFT_ERROR_INVALID_ARGUMENT: return "invalid argument";
+    case DRIFT_ERROR_CUDA: return "CUDA error";
+    case DRIFT_ERROR_WORKSPACE: return "workspace too small";
+    case DRIFT_ERROR_NO_DEVICE: return "no CUDA device";
+    case DRIFT_ERROR_OUT_OF_MEMORY: return "out of device memory";
+    default: return "unknown error";
+    }
+}
+
+const char *drift_last_error(void) { return g_last_error.c_str(); }
+
+// Series / continued-fraction lower incomplete gamma (Numerical Recipes 3rd
+// ed. section 6.2), host copy used to normalise the bulge.
+static double host_lower_gamma(double s, double x, double gamma_s)
+{
+    const double eps = 1.1102230246251565e-16;
+    const double fpmin = 1e-300;
+    if (!(x > 0.0)) return 0.0;
+    double prefactor = std::exp(s * std::log(x) - x);
+    if (x < s + 1.0) {
+        double ap = s, del = 1.0 / s, sum = del;
+        for (int n = 0; n < 500; ++n) {
+            ap += 1.0;
+            del *= x / ap;
+            sum += del;
+            if (std::fabs(del) < std::fabs(sum) * eps) break;
+        }
+        return sum * prefactor;
+    }
+    double b = x + 1.0 - s, c = 1.0 / fpmin, d = 1.0 / b, h = d;
+    for (int i = 1; i < 500; ++i) {
+        double an = -i * (i - s);
+        b += 2.0;
+        d = an * d + b;
+        if (std::fabs(d) < fpmin) d = fpmin;
+        c = b + an / c;
+        if (std::fabs(c) < fpmin) c = fpmin;
+        d = 1.0 / d;
+        double del = d * c;
+        h *= del;
+        if (std::fabs(del - 1.0) < eps) break;
+    }
+    return gamma_s - prefactor * h;
+}
+
+int drift_potential_bovy(drift_potential *p, double alpha, double rc, double bulge_force_at_1,
+                         double mn_amp, double mn_a, double mn_b, double nfw_amp, double nfw_a)
+{
+    if (!p) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "potential is NULL");
+    if (!(alpha < 3.0) || !(rc > 0.0) || !is_finite_value(bulge_force_at_1))
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "bulge needs alpha < 3, rc > 0 and a finite force");
+    std::memset(p, 0, sizeof(*p));
+    p->kind = DRIFT_POT_BOVY;
+    p->bulge_alpha = alpha;
+    p->bulge_rc = rc;
+    double s = 1.5 - 0.5 * alpha;
+    p->bulge_gamma_s = std::tgamma(s);
+    p->bulge_k = bulge_force_at_1 / host_lower_gamma(s, 1.0 / (rc * rc), p->bulge_gamma_s);
+    p->mn_amp = mn_amp;
+    p->mn_a = mn_a;
+    p->mn_b = mn_b;
+    p->nfw_amp = nfw_amp;
+    p->nfw_a = nfw_a;
+    return DRIFT_SUCCESS;
+}
+
+int drift_query_workspace(const drift_launch *launch, size_t *bytes)
+{
+    if (!launch || !bytes) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument");
+    *bytes = launch->schedule == DRIFT_SCHEDULE_PERSISTENT ? CURSOR_BYTES : 0;
+    return DRIFT_SUCCESS;
+}
+
+int drift_integrate(const drift_launch *launch, void *stream)
+{
+    int rc = validate(launch, true);
+    if (rc) return rc;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    if (launch->schedule == DRIFT_SCHEDULE_PERSISTENT) {
+        if (!launch->workspace || launch->workspace_bytes < sizeof(unsigned long long) ||
+            reinterpret_cast<uintptr_t>(launch->workspace) % 8)
+            return fail(DRIFT_ERROR_WORKSPACE, "persistent schedule needs an 8-byte aligned workspace of at least 8 bytes");
+    }
+    return launch_device(ctx, launch, launch->workspace, static_cast<cudaStream_t>(stream));
+}
+
+int drift_host_alloc(size_t bytes, void **ptr)
+{
+    if (!ptr) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "ptr is NULL");
+    cudaError_t e = cudaMallocHost(ptr, bytes ? bytes : 1);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+    return DRIFT_SUCCESS;
+}
+
+int drift_host_free(void *ptr)
+{
+    cudaError_t e = cudaFreeHost(ptr);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaFreeHost");
+    return DRIFT_SUCCESS;
+}
+
+int drift_integrate_host(const drift_launch *L)
+{
+    int rc = validate(L, false);
+    if (rc) return rc;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+
+    const int64_t n = L->n;
+    const int64_t nt = L->nt;
+    const size_t row = 6 * sizeof(double);
+
+    // Whole-request buffers: initial states, grid, per-particle outputs.
+    DRIFT_CUDA_TRY(ctx->y0.ensure(n * row), "cudaMalloc(y0)");
+    const size_t grid_bytes = L->ts ? nt * sizeof(double) : n * sizeof(double);
+    DRIFT_CUDA_TRY(ctx->grid.ensure(grid_bytes), "cudaMalloc(grid)");
+    if (L->y_final) DRIFT_CUDA_TRY(ctx->yfin.ensure(n * row), "cudaMalloc(y_final)");
+    if (L->status) DRIFT_CUDA_TRY(ctx->status.ensure(n), "cudaMalloc(status)");
+    if (L->err_code) DRIFT_CUDA_TRY(ctx->err.ensure(n * sizeof(int32_t)), "cudaMalloc(err)");
+    if (L->n_accepted) DRIFT_CUDA_TRY(ctx->acc.ensure(n * sizeof(uint32_t)), "cudaMalloc(acc)");
+    if (L->n_rejected) DRIFT_CUDA_TRY(ctx->rej.ensure(n * sizeof(uint32_t)), "cudaMalloc(rej)");
+    DRIFT_CUDA_TRY(ctx->cursor.ensure(2 * CURSOR_BYTES), "cudaMalloc(cursor)");
+
+    // Trajectory chunks: particles [c0, c0 + cn) write a (nt, cn, 6) device
+    // block that is copied out row by row into the caller's (nt, n, 6) array.
+    int64_t chunk = n;
+    if (L->out) {
+        size_t free_b = 0, total_b = 0;
+        DRIFT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+        const size_t budget = std::min<size_t>(free_b / 4, size_t(8) << 30);
+        int64_t by_mem = (int64_t)(budget / (nt * row));
+        // at least two chunks when the output is large so copies overlap compute
+        int64_t target = n > 65536 ? (n + 3) / 4 : n;
+        chunk = std::max<int64_t>(1, std::min(target, by_mem));
+        if (chunk < n) chunk = std::max<int64_t>(128, chunk / 128 * 128);
+        chunk = std::min(chunk, n);
+        for (int i = 0; i < 2; i++)
+            DRIFT_CUDA_TRY(ctx->out[i].ensure(chunk * nt * row), "cudaMalloc(out chunk)");
+    }
+    const bool out_pinned = L->out && is_pinned(L->out);
+    if (L->out && !out_pinned)
+        for (int i = 0; i < 2; i++)
+            DRIFT_CUDA_TRY(ctx->stage[i].ensure(chunk * nt * row), "cudaMallocHost(stage)");
+
+    cudaStream_t s0 = ctx->streams[0];
+    DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->y0.ptr, L->y0, n * row, cudaMemcpyHostToDevice, s0), "H2D y0");
+    DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->grid.ptr, L->ts ? (const void *)L->ts : (const void *)L->t_end,
+                                   grid_bytes, cudaMemcpyHostToDevice, s0),
+                   "H2D grid");
+    DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[0], s0), "cudaEventRecord");
+    DRIFT_CUDA_TRY(cudaStreamWaitEvent(ctx->streams[1], ctx->done[0], 0), "cudaStreamWaitEvent");
+
+    int64_t chunk_index = 0;
+    int64_t pending_c0[2] = {-1, -1}, pending_cn[2] = {0, 0};
+    auto drain_stage = [&](int slot) -> int {
+        // Move a finished pageable-destination chunk from pinned staging.
+        if (pending_c0[slot] < 0) return DRIFT_SUCCESS;
+        DRIFT_CUDA_TRY(cudaEventSynchronize(ctx->done[slot]), "cudaEventSynchronize");
+        const int64_t c0 = pending_c0[slot], cn = pending_cn[slot];
+        const char *src = static_cast<const char *>(ctx->stage[slot].ptr);
+        char *dst = reinterpret_cast<char *>(L->out);
+        for (int64_t k = 0; k < nt; k++)
+            std::memcpy(dst + (k * n + c0) * row, src + k * cn * row, cn * row);
+        pending_c0[slot] = -1;
+        return DRIFT_SUCCESS;
+    };
+
+    for (int64_t c0 = 0; c0 < n; c0 += chunk, chunk_index++) {
+        const int slot = (int)(chunk_index & 1);
+        cudaStream_t s = ctx->streams[slot];
+        const int64_t cn = std::min(chunk, n - c0);
+        if (L->out && !out_pinned) {
+            rc = drain_stage(slot);
+            if (rc) return rc;
+        }
+        drift_launch sub = *L;
+        sub.n = cn;
+        sub.y0 = ctx->y0.as<double>() + c0 * 6;
+        sub.ts = L->ts ? ctx->grid.as<double>() : nullptr;
+        sub.t_end = L->ts ? nullptr : ctx->grid.as<double>() + c0;
+        sub.out = L->out ? ctx->out[slot].as<double>() : nullptr;
+        sub.y_final = L->y_final ? ctx->yfin.as<double>() + c0 * 6 : nullptr;
+        sub.status = L->status ? ctx->status.as<uint8_t>() + c0 : nullptr;
+        sub.err_code = L->err_code ? ctx->err.as<int32_t>() + c0 : nullptr;
+        sub.n_accepted = L->n_accepted ? ctx->acc.as<uint32_t>() + c0 : nullptr;
+        sub.n_rejected = L->n_rejected ? ctx->rej.as<uint32_t>() + c0 : nullptr;
+        rc = launch_device(ctx, &sub, static_cast<char *>(ctx->cursor.ptr) + slot * CURSOR_BYTES, s);
+        if (rc) return rc;
+        if (L->out) {
+            if (out_pinned) {
+                DRIFT_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<char *>(L->out) + c0 * row, n * row,
+                                                 sub.out, cn * row, cn * row, nt,
+                                                 cudaMemcpyDeviceToHost, s),
+                               "D2H trajectories");
+            } else {
+                DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->stage[slot].ptr, sub.out, cn * nt * row,
+                                               cudaMemcpyDeviceToHost, s),
+                               "D2H trajectories");
+                DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[slot], s), "cudaEventRecord");
+                pending_c0[slot] = c0;
+                pending_cn[slot] = cn;
+            }
+        }
+    }
+    for (int slot = 0; slot < 2; slot++) {
+        if (L->out && !out_pinned) {
+            rc = drain_stage(slot);
+            if (rc) return rc;
+        }
+    }
+    // Per-particle outputs once every chunk is done.
+    DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[1], ctx->streams[1]), "cudaEventRecord");
+    DRIFT_CUDA_TRY(cudaStreamWaitEvent(s0, ctx->done[1], 0), "cudaStreamWaitEvent");
+    if (L->y_final)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->y_final, ctx->yfin.ptr, n * row, cudaMemcpyDeviceToHost, s0), "D2H y_final");
+    if (L->status)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->status, ctx->status.ptr, n, cudaMemcpyDeviceToHost, s0), "D2H status");
+    if (L->err_code)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->err_code, ctx->err.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s0), "D2H err");
+    if (L->n_accepted)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->n_accepted, ctx->acc.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s0), "D2H accepted");
+    if (L->n_rejected)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->n_rejected, ctx->rej.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s0), "D2H rejected");
+    DRIFT_CUDA_TRY(cudaStreamSynchronize(s0), "cudaStreamSynchronize");
+    DRIFT_CUDA_TRY(cudaStreamSynchronize(ctx->streams[1]), "cudaStreamSynchronize");
+    return DRIFT_SUCCESS;
+}
+
+int drift_galpy_dopr54(const double *state0, const double *times, double *state_out, int64_t n,
+                       int64_t nt, double rtol, double atol, double dt_one_init, void *stream)
+{
+    drift_launch L;
+    std::memset(&L, 0, sizeof(L));
+    L.method = DRIFT_DOPR54;
+    L.precision = DRIFT_PRECISION_EXACT;
+    L.schedule = DRIFT_SCHEDULE_PLAIN;
+    L.potential.kind = DRIFT_POT_KEPLER;
+    L.potential.amp = 1.0;
+    L.n = n;
+    L.y0 = state0;
+    L.nt = nt;
+    L.ts = times;
+    L.out = state_out;
+    L.rtol_ln = rtol;
+    L.atol_ln = atol;
+    L.dt_one = dt_one_init;
+    return drift_integrate(&L, stream);
+}
+
+int drift_galpy_dop853(const double *state0, const double *times, double *state_out, int64_t n,
+                       int64_t nt, double rtol, double atol, void *stream)
+{
+    drift_launch L;
+    std::memset(&L, 0, sizeof(L));
+    L.method = DRIFT_DOP853;
+    L.precision = DRIFT_PRECISION_EXACT;
+    L.schedule = DRIFT_SCHEDULE_PLAIN;
+    L.potential.kind = DRIFT_POT_KEPLER;
+    L.potential.amp = 1.0;
+    L.n = n;
+    L.y0 = state0;
+    L.nt = nt;
+    L.ts = times;
+    L.out = state_out;
+    L.rtol_ln = rtol;
+    L.atol_ln = atol;
+    L.dt_one = DRIFT_INITIAL_STEP_SENTINEL;
+    return drift_integrate(&L, stream);
+}
+
+}  // extern "C"

@@ -1,0 +1,62 @@
+// drift_common.cuh -- small shared pieces of the integrator kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "drift_math.cuh"
+#include "drift_potentials.cuh"
+
+namespace drift {
+
+// dop853.rs:286-299: comparisons without fmin/fmax NaN semantics.
+__device__ __forceinline__ double c_min(double a, double b) { return a < b ? a : b; }
+__device__ __forceinline__ double c_max(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double custom_sign(double x, double y)
+{
+    return y > 0.0 ? fabs(x) : -fabs(x);
+}
+
+// Output grid of one particle: either a shared array of nt times, or the
+// uniform grid t0..t_end with nt points sampled as OutputGrid::sample does
+// (shared/src/config.rs:57-66; exact end point).
+struct Grid {
+    const double *ts;
+    double t0, t_end;
+    int32_t nt;
+    __device__ __forceinline__ double at(int32_t k) const
+    {
+        if (ts) return __ldg(ts + k);
+        if (k == nt - 1) return t_end;
+        return t0 + (t_end - t0) * (double)k / (double)(nt - 1);
+    }
+};
+
+// Writes one 6-vector of particle `pid` at output slot k of a time-major
+// (nt, n, 6) array with 16-byte vector stores (48 B per sample, aligned).
+struct TimeMajorOut {
+    double *base;  // NULL: trajectories not requested
+    int64_t n;
+    int64_t pid;
+    double last[6];  // most recent sample (the final state once done)
+    __device__ __forceinline__ void write(int32_t k, const double *v)
+    {
+#pragma unroll
+        for (int i = 0; i < 6; i++) last[i] = v[i];
+        if (base) {
+            double2 *p = reinterpret_cast<double2 *>(base + ((int64_t)k * n + pid) * 6);
+            __stcs(p + 0, make_double2(v[0], v[1]));
+            __stcs(p + 1, make_double2(v[2], v[3]));
+            __stcs(p + 2, make_double2(v[4], v[5]));
+        }
+    }
+};
+
+__device__ __forceinline__ uint64_t global_timer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+}  // namespace drift

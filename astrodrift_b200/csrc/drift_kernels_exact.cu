@@ -1,0 +1,16 @@
+// Integration kernels without multiply-add contraction (compiled -fmad=false):
+// the stage arithmetic rounds exactly as the reference's Rust code does.
+#define DRIFT_PRECISION_NS exact
+#include "drift_kernels.cuh"
+
+namespace drift {
+cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
+                         cudaStream_t stream)
+{
+    return exact::launch_impl(a, method, grid, block, stream);
+}
+cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)
+{
+    return exact::occupancy_impl(method, kind, block, blocks_per_sm);
+}
+}  // namespace drift

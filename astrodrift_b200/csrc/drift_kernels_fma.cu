@@ -1,0 +1,15 @@
+// Integration kernels with multiply-add contraction (compiled -fmad=true).
+#define DRIFT_PRECISION_NS fma_mode
+#include "drift_kernels.cuh"
+
+namespace drift {
+cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
+                       cudaStream_t stream)
+{
+    return fma_mode::launch_impl(a, method, grid, block, stream);
+}
+cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm)
+{
+    return fma_mode::occupancy_impl(method, kind, block, blocks_per_sm);
+}
+}  // namespace drift

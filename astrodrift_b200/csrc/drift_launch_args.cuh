@@ -1,0 +1,44 @@
+// drift_launch_args.cuh -- parameter block shared by the kernels and the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "drift_b200.h"
+#include "drift_dopr54.cuh"
+
+namespace drift {
+
+// Everything a launch needs, passed by value as the kernel parameter.
+struct KernelArgs {
+    int64_t n;
+    const double *y0;         // (n, 6)
+    int32_t nt;
+    int32_t persistent;       // 0: plain schedule, 1: persistent schedule
+    const double *ts;         // shared grid or NULL
+    double t0;                // per-particle grid start
+    const double *t_end;      // per-particle grid end (when ts == NULL)
+    double *out;              // (nt, n, 6) or NULL
+    double *y_final;          // (n, 6) or NULL
+    double rtol, atol;        // DOP853: exp(ln tolerance), formed on the host
+    Dopr54Tol tol54;          // DOPR54: exp(ln tolerance), formed on the host
+    double dt_one;            // DOPR54 first step or the estimate sentinel
+    int64_t max_steps;
+    uint64_t timeout_ns;      // per-thread device-time budget from its start, 0 = none
+    uint8_t *status;
+    int32_t *err_code;
+    uint32_t *n_accepted;
+    uint32_t *n_rejected;
+    unsigned long long *cursor;  // persistent schedule queue position (workspace)
+    drift_potential potential;
+};
+
+// Per-precision launchers (one translation unit each).
+cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
+                         cudaStream_t stream);
+cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
+                       cudaStream_t stream);
+cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm);
+cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm);
+
+}  // namespace drift

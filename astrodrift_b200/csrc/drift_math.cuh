@@ -1,0 +1,105 @@
+// drift_math.cuh -- FP64 special powers used on the integration path.
+//
+// The reference evaluates pow(r2, -1.5) in every force call, pow(err, 1/8) in
+// the DOP853 controller and pow(x, 1.5) in the Miyamoto-Nagai disk, all
+// through glibc's pow, which returns the correctly rounded result except in
+// rare near-halfway cases.  These routines compute the same powers from IEEE
+// sqrt and division plus one Newton correction carried in double-double
+// (two-term) arithmetic, so the result is the correctly rounded value unless
+// the exact power lies within about 2^-50 ulp of a rounding boundary.  They
+// are written from the algebra below; no vendor math code is reproduced.
+//
+//   x^(3/2):  s = RN(sqrt x), e = x - s^2 exactly (one fma), so
+//             sqrt x = s + e/(2s) + O(e^2) and x^(3/2) = x s + x e/(2s)
+//             = x s + e s / 2 (1 + O(2^-52)).
+//   x^(-3/2): r = 1 / x^(3/2) refined as r = rh (1 + (1 - rh (ph + pl))).
+//   x^(1/8):  y0 = sqrt(sqrt(sqrt x)) is within about one ulp; one Newton
+//             step on y^8 = x with y0^8 formed in double-double gives
+//             y = y0 (1 - (y0^8 - x) / (8 x)).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+namespace drift {
+
+// Exact product: a * b == hi + lo.
+__device__ __forceinline__ void two_prod(double a, double b, double &hi, double &lo)
+{
+    hi = a * b;
+    lo = fma(a, b, -hi);
+}
+
+// x^(3/2) as an unevaluated sum hi + lo, valid for x in [1e-200, 1e200].
+__device__ __forceinline__ void pow_1p5_dd(double x, double &hi, double &lo)
+{
+    double s = sqrt(x);
+    double e = fma(-s, s, x);
+    two_prod(x, s, hi, lo);
+    lo = fma(0.5 * e, s, lo);
+}
+
+__device__ __forceinline__ bool in_fast_range(double x)
+{
+    return x > 1e-200 && x < 1e200;
+}
+
+// x^(3/2), rounded to nearest (pow(x, 1.5) semantics for x >= 0).
+__device__ __forceinline__ double pow_1p5(double x)
+{
+    if (in_fast_range(x)) {
+        double hi, lo;
+        pow_1p5_dd(x, hi, lo);
+        return hi + lo;
+    }
+    if (x == 0.0) return 0.0;
+    if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);  // NaN
+    if (isinf(x)) return x;
+    // Rescale by an even power of two: x = m 4^k, x^(3/2) = m^(3/2) 8^k.
+    int k = (ilogb(x)) / 2;
+    double m = scalbn(x, -2 * k);
+    double hi, lo;
+    pow_1p5_dd(m, hi, lo);
+    return scalbn(hi + lo, 3 * k);
+}
+
+__device__ __forceinline__ double pow_m1p5_core(double x)
+{
+    double ph, pl;
+    pow_1p5_dd(x, ph, pl);
+    double rh = 1.0 / ph;
+    double eps = fma(-rh, ph, 1.0) - rh * pl;
+    return fma(rh, eps, rh);
+}
+
+// x^(-3/2), rounded to nearest (pow(x, -1.5) semantics, including the
+// special values: +-0 -> +inf, +inf -> +0, x < 0 -> NaN).
+__device__ __forceinline__ double pow_m1p5(double x)
+{
+    if (in_fast_range(x)) return pow_m1p5_core(x);
+    if (x == 0.0) return __longlong_as_double(0x7ff0000000000000LL);  // +inf
+    if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);
+    if (isinf(x)) return 0.0;
+    int k = (ilogb(x)) / 2;
+    double m = scalbn(x, -2 * k);
+    return scalbn(pow_m1p5_core(m), -3 * k);
+}
+
+// x^(1/8), rounded to nearest (pow(x, 0.125) semantics for the values the
+// controller produces: 0 -> 0, +inf -> +inf, NaN and x < 0 -> NaN).
+__device__ __forceinline__ double root8(double x)
+{
+    double y0 = sqrt(sqrt(sqrt(x)));
+    if (!(x > 1e-280 && x < 1e300)) return y0;
+    double a_h, a_l, b_h, b_l, c_h, c_l;
+    two_prod(y0, y0, a_h, a_l);                 // y0^2
+    two_prod(a_h, a_h, b_h, b_l);               // y0^4
+    b_l = fma(2.0 * a_h, a_l, b_l);
+    two_prod(b_h, b_h, c_h, c_l);               // y0^8
+    c_l = fma(2.0 * b_h, b_l, c_l);
+    double delta = ((c_h - x) + c_l) / x;       // y0^8 / x - 1
+    return fma(y0, -0.125 * delta, y0);
+}
+
+}  // namespace drift

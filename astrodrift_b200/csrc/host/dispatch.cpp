@@ -1,0 +1,252 @@
+// dispatch.cpp -- stage dispatch to the GPU through the C ABI.
+//
+// Restates gpu_dispatch / launch_kernel / dispatch_stages
+// (src/dispatch/gpu.rs:157-229, src/dispatch/mod.rs:14-34): log the request,
+// integrate each state-bearing stage in dependency order, return time-major
+// (nt, N, 6) trajectories.  Differences from the reference, by design:
+//  * the stage force comes from the model: the stationary background
+//    potential the stage requires (the reference ignores the model and always
+//    integrates a unit Kepler mass, src/dispatch/gpu.rs:155-156); potentials
+//    attached to moving particle groups are not yet force sources;
+//  * per-particle failures (galpy's DOPR54 error code, step cap, timeout)
+//    raise IntegrationError, as the reference's CPU path does for DOPR54
+//    (src/dispatch/cpu.rs:35-38, src/dispatch/mod.rs:74-75);
+//  * the GIL is released while the device works.
+#include "dispatch.h"
+
+#include <chrono>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+#include "drift_b200.h"
+
+namespace py = pybind11;
+
+namespace drift_host {
+
+namespace {
+
+const char *LOG_GPU = "drift.dispatch.gpu";
+const char *LOG_BACKEND = "drift.dispatch.gpu.b200";
+
+std::string fmt(const char *f, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, f);
+    vsnprintf(buf, sizeof(buf), f, ap);
+    va_end(ap);
+    return buf;
+}
+
+// Rust's `{}` for f64: shortest text that round-trips, integers without ".0".
+std::string rust_float(double v)
+{
+    if (std::isfinite(v) && v == std::floor(v) && std::fabs(v) < 1e16) return fmt("%.0f", v);
+    for (int p = 1; p <= 17; p++) {
+        std::string s = fmt("%.*g", p, v);
+        if (std::strtod(s.c_str(), nullptr) == v) return s;
+    }
+    return fmt("%.17g", v);
+}
+
+// Rust's `{:.3?}` for a Duration.
+std::string rust_duration(double seconds)
+{
+    if (seconds >= 1.0) return fmt("%.3fs", seconds);
+    if (seconds >= 1e-3) return fmt("%.3fms", seconds * 1e3);
+    if (seconds >= 1e-6) return fmt("%.3fus", seconds * 1e6);
+    return fmt("%.3fns", seconds * 1e9);
+}
+
+drift_potential potential_of(const Recipe &r)
+{
+    drift_potential p;
+    std::memset(&p, 0, sizeof(p));
+    switch (r.name) {
+    case PotentialName::Kepler:
+    case PotentialName::CustomKepler:
+        p.kind = DRIFT_POT_KEPLER;
+        p.amp = r.amp;
+        break;
+    case PotentialName::Plummer:
+    case PotentialName::CustomPlummer:
+        p.kind = DRIFT_POT_PLUMMER;
+        p.amp = r.amp;
+        p.b = r.radius;
+        break;
+    case PotentialName::Bovy:
+        if (drift_potential_bovy(&p, r.bulge_alpha, r.bulge_rc, r.bulge_force, r.mn_amp, r.mn_a,
+                                 r.mn_b, r.nfw_amp, r.nfw_a) != DRIFT_SUCCESS)
+            throw py::value_error(std::string("invalid Bovy parameters: ") + drift_last_error());
+        break;
+    }
+    return p;
+}
+
+const char *status_name(int s)
+{
+    switch (s) {
+    case DRIFT_PARTICLE_MIN_STEP: return "minimum step reached";
+    case DRIFT_PARTICLE_MAX_STEPS: return "step limit reached";
+    case DRIFT_PARTICLE_NONFINITE: return "non-finite error estimate";
+    case DRIFT_PARTICLE_TIMEOUT: return "device time budget exhausted";
+    default: return "ok";
+    }
+}
+
+}  // namespace
+
+[[noreturn]] void raise_not_implemented(const std::string &msg)
+{
+    PyErr_SetString(PyExc_NotImplementedError, msg.c_str());
+    throw py::error_already_set();
+}
+
+void log_record(const char *logger_name, int level, const char *file, int line, const std::string &msg)
+{
+    py::object logging = py::module_::import("logging");
+    py::object logger = logging.attr("getLogger")(logger_name);
+    if (!logger.attr("isEnabledFor")(level).cast<bool>()) return;
+    try {
+        py::object rec = logger.attr("makeRecord")(logger_name, level, file, line, msg, py::tuple(),
+                                                   py::none());
+        logger.attr("handle")(rec);
+    } catch (py::error_already_set &e) {
+        e.discard_as_unraisable(py::str("drift logging handler"));
+    }
+}
+
+#define DRIFT_LOG(logger, level, msg) log_record(logger, level, "gpu_dispatch.cpp", __LINE__, msg)
+
+std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const IntegrationPlan &plan,
+                                              std::vector<StageStats> *stats)
+{
+    const OutputGrid &ts = config.output;
+    DRIFT_LOG(LOG_GPU, LOG_INFO,
+              fmt("GPU integration starting: implementation=%s, method=%s, %lld output times over [%s, %s], rtol=%.2e, atol=%.2e",
+                  name_of(config.implementation), name_of(config.method), (long long)ts.steps,
+                  rust_float(ts.start).c_str(), rust_float(ts.end).c_str(), config.tolerance.rtol,
+                  config.tolerance.atol));
+    const auto started = std::chrono::steady_clock::now();
+
+    std::vector<double> times(ts.steps);
+    for (int64_t i = 0; i < ts.steps; i++) times[i] = ts.sample(i);
+
+    // LogTolerance::from_linear (src/integrators/galpy/mod.rs:19-24)
+    const double rtol_ln = std::log(config.tolerance.rtol);
+    const double atol_ln = std::log(config.tolerance.atol);
+
+    std::vector<py::array_t<double>> results;
+    int64_t total_particles = 0;
+    static bool backend_announced = false;
+    int stage_no = 0;
+    for (const Stage &stage : plan.stages) {
+        stage_no++;
+        const Container &c = *stage.container;
+        const int64_t n = *c.num_particles;
+        total_particles += n;
+        DRIFT_LOG(LOG_GPU, LOG_DEBUG, fmt("stage %d: dispatching %lld particles to the GPU", stage_no, (long long)n));
+
+        std::vector<const Recipe *> backgrounds;
+        for (size_t i = 0; i < stage.recipes.size(); i++)
+            if (stage.recipe_is_background[i]) backgrounds.push_back(&stage.recipes[i]);
+        if (backgrounds.size() != 1)
+            raise_not_implemented(fmt(
+                "stage %d requires %zu stationary background potentials; the GPU path integrates "
+                "exactly one (potentials attached to particle groups are not yet force sources)",
+                stage_no, backgrounds.size()));
+
+        drift_launch L;
+        std::memset(&L, 0, sizeof(L));
+        L.method = config.method == Method::DOPR54 ? DRIFT_DOPR54 : DRIFT_DOP853;
+        L.precision = config.precision == Precision::EXACT ? DRIFT_PRECISION_EXACT : DRIFT_PRECISION_FMA;
+        L.schedule = config.schedule == Schedule::PLAIN ? DRIFT_SCHEDULE_PLAIN : DRIFT_SCHEDULE_PERSISTENT;
+        L.block_size = config.block_size;
+        L.potential = potential_of(*backgrounds[0]);
+        L.n = n;
+        L.y0 = c.state->data();
+        L.nt = ts.steps;
+        if (c.t_end) {
+            L.ts = nullptr;
+            L.t0 = ts.start;
+            L.t_end = c.t_end->data();
+        } else {
+            L.ts = times.data();
+        }
+        L.rtol_ln = rtol_ln;
+        L.atol_ln = atol_ln;
+        L.dt_one = DRIFT_INITIAL_STEP_SENTINEL;
+        L.max_steps = config.max_steps;
+        L.timeout_s = config.timeout_s;
+
+        py::array_t<double> out({(py::ssize_t)ts.steps, (py::ssize_t)n, (py::ssize_t)STATE_DIM});
+        py::array_t<uint8_t> status(n);
+        py::array_t<int32_t> err(n);
+        py::array_t<uint32_t> acc(n), rej(n);
+        L.out = out.mutable_data();
+        L.status = status.mutable_data();
+        L.err_code = err.mutable_data();
+        L.n_accepted = acc.mutable_data();
+        L.n_rejected = rej.mutable_data();
+
+        const char *kernel_label = config.method == Method::DOPR54 ? "GALPY DOPR54" : "GALPY DOP853";
+        DRIFT_LOG(LOG_GPU, LOG_DEBUG,
+                  fmt("launching %s kernel: %lld particles, block=%d, schedule=%s, %lld output times",
+                      kernel_label, (long long)n, config.block_size ? config.block_size : 128,
+                      config.schedule == Schedule::PLAIN ? "plain" : "persistent", (long long)ts.steps));
+        if (!backend_announced) {
+            DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, "context initialized and kernel module loaded (sm_100a)");
+            backend_announced = true;
+        }
+        const size_t in_bytes = n * STATE_DIM * sizeof(double) +
+                                (c.t_end ? n : ts.steps) * sizeof(double);
+        DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, fmt("copying %zu bytes of host data to the device", in_bytes));
+
+        const auto stage_started = std::chrono::steady_clock::now();
+        int rc;
+        {
+            py::gil_scoped_release nogil;
+            rc = drift_integrate_host(&L);
+        }
+        const double secs =
+            std::chrono::duration<double>(std::chrono::steady_clock::now() - stage_started).count();
+        if (rc != DRIFT_SUCCESS) {
+            std::string why = drift_last_error();
+            if (rc == DRIFT_ERROR_NO_DEVICE) throw DriftErrorCpp("GPU integration needs a CUDA device: " + why);
+            throw IntegrationErrorCpp(fmt("GPU %s integration failed: %s (%s)", name_of(config.method),
+                                          drift_result_string(rc), why.c_str()));
+        }
+        const size_t out_bytes = (size_t)ts.steps * n * STATE_DIM * sizeof(double);
+        DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, fmt("copied %zu result bytes to the host", out_bytes));
+
+        // galpy's DOPR54 error code first (the reference's CPU error), then
+        // the build's own per-particle limits.
+        const int32_t *e = err.data();
+        const uint8_t *s = status.data();
+        for (int64_t i = 0; i < n; i++)
+            if (e[i] != 0)
+                throw IntegrationErrorCpp(fmt("GPU %s integration failed with error code %d (particle %lld)",
+                                              name_of(config.method), e[i], (long long)i));
+        for (int64_t i = 0; i < n; i++)
+            if (s[i] != DRIFT_PARTICLE_OK)
+                throw IntegrationErrorCpp(fmt("GPU %s integration failed for particle %lld: %s",
+                                              name_of(config.method), (long long)i, status_name(s[i])));
+
+        DRIFT_LOG(LOG_GPU, LOG_DEBUG,
+                  fmt("stage %d: %lld particles finished in %s", stage_no, (long long)n,
+                      rust_duration(secs).c_str()));
+        results.push_back(out);
+        if (stats) stats->push_back(StageStats{acc, rej, status, secs});
+    }
+    const double elapsed =
+        std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();
+    DRIFT_LOG(LOG_GPU, LOG_INFO,
+              fmt("GPU integration finished: %d stage(s), %lld particle trajectories in %s", stage_no,
+                  (long long)total_particles, rust_duration(elapsed).c_str()));
+    return results;
+}
+
+}  // namespace drift_host

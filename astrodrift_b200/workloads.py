@@ -1,0 +1,88 @@
+"""Seeded synthetic initial conditions for the benchmark configurations.
+
+No public dataset is involved: every workload is drawn from a fixed-seed
+numpy generator with the distributions the configurations specify.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+
+def _isotropic(rng, n):
+    u = rng.normal(size=(n, 3))
+    return u / np.linalg.norm(u, axis=1, keepdims=True)
+
+
+def plummer_sphere(n: int, seed: int = 2, amp: float = 1.0, b: float = 1.0,
+                   u_cap: float = 0.999) -> np.ndarray:
+    """Isotropic Plummer distribution function (G = 1).
+
+    Radius by inverse CDF, r = b / sqrt(u^(-2/3) - 1) with u ~ U(0, u_cap];
+    speed q * v_esc with q drawn by rejection from g(q) = q^2 (1 - q^2)^(7/2)
+    under the bound 0.1 (Aarseth, Henon & Wielen 1974); isotropic directions.
+    """
+    rng = np.random.default_rng(seed)
+    u = rng.uniform(0.0, u_cap, n)
+    u = np.where(u == 0.0, u_cap, u)
+    r = b / np.sqrt(u ** (-2.0 / 3.0) - 1.0)
+    q = np.empty(n)
+    filled = 0
+    while filled < n:
+        m = 2 * (n - filled) + 64
+        x = rng.uniform(0.0, 1.0, m)
+        y = rng.uniform(0.0, 0.1, m)
+        acc = x[y < x * x * (1.0 - x * x) ** 3.5]
+        take = min(len(acc), n - filled)
+        q[filled:filled + take] = acc[:take]
+        filled += take
+    v_esc = np.sqrt(2.0 * amp / np.sqrt(r * r + b * b))
+    pos = _isotropic(rng, n) * r[:, None]
+    vel = _isotropic(rng, n) * (q * v_esc)[:, None]
+    return np.ascontiguousarray(np.hstack([pos, vel]))
+
+
+def kepler_disc(n: int, seed: int = 1) -> np.ndarray:
+    """Configuration 1: r ~ U[0.5, 2], isotropic orbital plane, tangential
+    speed sqrt(1/r) U[0.9, 1.1], radial speed N(0, 0.05 sqrt(1/r)); draws with
+    cylindrical radius < 1e-3 are redrawn (the galpy Kepler force is singular
+    on the z axis)."""
+    rng = np.random.default_rng(seed)
+    out = np.empty((n, 6))
+    filled = 0
+    while filled < n:
+        m = n - filled
+        r = rng.uniform(0.5, 2.0, m)
+        normal = _isotropic(rng, m)
+        a = _isotropic(rng, m)
+        rhat = np.cross(normal, a)
+        rhat /= np.linalg.norm(rhat, axis=1, keepdims=True)
+        that = np.cross(normal, rhat)
+        vt = np.sqrt(1.0 / r) * rng.uniform(0.9, 1.1, m)
+        vr = rng.normal(0.0, 0.05 * np.sqrt(1.0 / r))
+        pos = rhat * r[:, None]
+        vel = that * vt[:, None] + rhat * vr[:, None]
+        ok = np.hypot(pos[:, 0], pos[:, 1]) >= 1e-3
+        k = int(ok.sum())
+        out[filled:filled + k] = np.hstack([pos, vel])[ok]
+        filled += k
+    return out
+
+
+def bovy_disc(n: int, seed: int = 3, radial_force=None) -> tuple[np.ndarray, np.ndarray]:
+    """Configuration 3: R log-uniform on [0.05, 20], phi ~ U[0, 2 pi),
+    z ~ N(0, 0.1 R); v_c(R) = sqrt(R |F_R(R, 0)|); v_T = v_c (1 + 0.1 N(0,1)),
+    v_R, v_z ~ N(0, 0.1 v_c); per-particle end times t_end ~ U[10, 1000].
+    `radial_force(R)` returns F_R(R, 0) of the composite."""
+    rng = np.random.default_rng(seed)
+    R = np.exp(rng.uniform(np.log(0.05), np.log(20.0), n))
+    phi = rng.uniform(0.0, 2.0 * np.pi, n)
+    z = rng.normal(0.0, 1.0, n) * 0.1 * R
+    vc = np.sqrt(R * np.abs(radial_force(R)))
+    vT = vc * (1.0 + 0.1 * rng.normal(size=n))
+    vR = 0.1 * vc * rng.normal(size=n)
+    vz = 0.1 * vc * rng.normal(size=n)
+    c, s = np.cos(phi), np.sin(phi)
+    y0 = np.stack([R * c, R * s, z, vR * c - vT * s, vR * s + vT * c, vz], axis=1)
+    t_end = rng.uniform(10.0, 1000.0, n)
+    return np.ascontiguousarray(y0), t_end

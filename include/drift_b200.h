@@ -1,0 +1,185 @@
+/*
+ * drift_b200.h -- C ABI of the B200 batched Dormand-Prince test-particle integrator.
+ *
+ * This is the host->device boundary of the lbparticles/astrodrift ("drift")
+ * integration path.  In the reference that boundary is the per-backend
+ *   backend::launch(kernel, input_state, times, output_state)
+ * (src/dispatch/gpu/cuda_oxide.rs:9-86, src/dispatch/gpu/rust_cuda.rs:10-91)
+ * calling the device kernels
+ *   galpy_dopr54(state0, times, state_out, n, nt, rtol, atol, dt_one_init)
+ *   galpy_dop853(state0, times, state_out, n, nt, rtol, atol)
+ * (kernels/src/lib.rs:143-173 and :188-216).  Every entry point below uses
+ * plain pointers and sizes only.  Tolerances are natural logarithms, exactly
+ * as the reference kernels receive them (src/integrators/galpy/mod.rs:19-24).
+ *
+ * Layouts: initial states are (n, 6) row-major [x, y, z, vx, vy, vz];
+ * trajectories are time-major (nt, n, 6), as write_time_major_state writes
+ * them (kernels/src/lib.rs:18-33).
+ *
+ * Threading: calls are thread-safe; device work is ordered on the stream the
+ * caller passes (NULL = the legacy default stream).
+ */
+#ifndef DRIFT_B200_H
+#define DRIFT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DRIFT_ABI_VERSION 1
+
+/* Sentinel that asks DOPR54 for galpy's RK4 initial-step estimate
+ * (src/integrators/galpy/mod.rs:8). */
+#define DRIFT_INITIAL_STEP_SENTINEL (-9999.99)
+
+typedef enum {
+    DRIFT_DOPR54 = 0, /* galpy bovy_rk.c DOPR54 (src/integrators/galpy/dopr54.rs) */
+    DRIFT_DOP853 = 1  /* galpy leung_dop853.c DOP853 (src/integrators/galpy/dop853.rs) */
+} drift_method;
+
+typedef enum {
+    /* galpy's cylindrical point-mass force, the force both reference
+     * integrators evaluate (src/integrators/galpy/dopr54.rs:75-88). */
+    DRIFT_POT_KEPLER = 0,
+    /* shared/src/potential.rs:241-262 */
+    DRIFT_POT_PLUMMER = 1,
+    /* bulge + Miyamoto-Nagai disk + NFW halo (shared/src/potential.rs:87-176),
+     * with a power-law-with-cutoff bulge */
+    DRIFT_POT_BOVY = 2,
+    /* KeplerPotential::force, Cartesian (shared/src/potential.rs:217-239) */
+    DRIFT_POT_KEPLER_CARTESIAN = 3
+} drift_potential_kind;
+
+typedef enum {
+    /* No multiply-add contraction: the stage arithmetic rounds exactly like
+     * the reference's Rust code (which never contracts). */
+    DRIFT_PRECISION_EXACT = 0,
+    /* Multiply-adds fused: fewer FP64 instructions, results differ from the
+     * reference at the last-bit level. */
+    DRIFT_PRECISION_FMA = 1
+} drift_precision;
+
+typedef enum {
+    /* One particle per thread for the life of the launch. */
+    DRIFT_SCHEDULE_PLAIN = 0,
+    /* Persistent grid; a thread that finishes its particle takes the next one
+     * from a device-wide cursor (needs workspace). */
+    DRIFT_SCHEDULE_PERSISTENT = 1
+} drift_schedule;
+
+/* Return codes of every entry point. */
+typedef enum {
+    DRIFT_SUCCESS = 0,
+    DRIFT_ERROR_INVALID_ARGUMENT = 1,
+    DRIFT_ERROR_CUDA = 2,
+    DRIFT_ERROR_WORKSPACE = 3,
+    DRIFT_ERROR_NO_DEVICE = 4,
+    DRIFT_ERROR_OUT_OF_MEMORY = 5
+} drift_result;
+
+/* Per-particle status codes written to drift_launch.status. */
+typedef enum {
+    DRIFT_PARTICLE_OK = 0,
+    /* DOPR54 hit galpy's minimum step (init/10^4) or a NaN step and forced an
+     * accept; galpy's error code is odd (src/integrators/galpy/dopr54.rs:407-418). */
+    DRIFT_PARTICLE_MIN_STEP = 1,
+    /* The max_steps cap ended the integration (the reference has no cap). */
+    DRIFT_PARTICLE_MAX_STEPS = 2,
+    /* DOP853's error estimate stayed non-finite for 64 consecutive attempts. */
+    DRIFT_PARTICLE_NONFINITE = 3,
+    /* The launch deadline passed before this particle finished. */
+    DRIFT_PARTICLE_TIMEOUT = 4
+} drift_particle_status;
+
+/* Potential descriptor.  Fields a kind does not use are ignored. */
+typedef struct {
+    int32_t kind;          /* drift_potential_kind */
+    int32_t reserved;
+    double amp;            /* Kepler / Plummer mass (G = 1) */
+    double b;              /* Plummer radius */
+    double mn_amp, mn_a, mn_b;   /* Miyamoto-Nagai disk */
+    double nfw_amp, nfw_a;       /* NFW halo */
+    double bulge_alpha;    /* bulge density slope, rho ~ r^-alpha exp(-(r/rc)^2) */
+    double bulge_rc;       /* bulge cutoff radius */
+    double bulge_k;        /* F_r = -bulge_k gamma(s, r^2/rc^2) / r^2, s = 1.5 - alpha/2 */
+    double bulge_gamma_s;  /* complete Gamma(s) */
+} drift_potential;
+
+/* One integration request.  Pointers are DEVICE pointers for drift_integrate
+ * and HOST pointers for drift_integrate_host. */
+typedef struct {
+    int32_t method;        /* drift_method */
+    int32_t precision;     /* drift_precision */
+    int32_t schedule;      /* drift_schedule */
+    int32_t block_size;    /* threads per block; 0 = library default */
+    drift_potential potential;
+    int64_t n;             /* particles, >= 1 */
+    const double *y0;      /* (n, 6) initial states */
+    int64_t nt;            /* output times per particle, >= 2 */
+    const double *ts;      /* (nt) shared output grid, or NULL ... */
+    double t0;             /* ... then particle i uses the nt-point uniform grid */
+    const double *t_end;   /*     t0 .. t_end[i] (shared/src/config.rs:57-66) */
+    double *out;           /* (nt, n, 6) trajectories, or NULL */
+    double *y_final;       /* (n, 6) state at the last output time, or NULL */
+    double rtol_ln;        /* ln(rtol) */
+    double atol_ln;        /* ln(atol) */
+    double dt_one;         /* DOPR54 first step; DRIFT_INITIAL_STEP_SENTINEL = estimate */
+    int64_t max_steps;     /* step attempts per particle before MAX_STEPS; <= 0 = 10^8 */
+    double timeout_s;      /* device-time budget of the launch; <= 0 = none */
+    uint8_t *status;       /* (n) drift_particle_status, or NULL */
+    int32_t *err_code;     /* (n) galpy DOPR54 error code, or NULL */
+    uint32_t *n_accepted;  /* (n) accepted steps, or NULL */
+    uint32_t *n_rejected;  /* (n) rejected steps, or NULL */
+    void *workspace;       /* device scratch for the persistent schedule */
+    size_t workspace_bytes;
+} drift_launch;
+
+/* Library / device information. */
+int drift_abi_version(void);
+const char *drift_result_string(int code);
+/* Message of the last failing call on this thread ("" if none). */
+const char *drift_last_error(void);
+
+/* Page-locked host memory for drift_integrate_host buffers: with pinned
+ * trajectory buffers the copy-out of one particle chunk overlaps the
+ * integration of the next. */
+int drift_host_alloc(size_t bytes, void **ptr);
+int drift_host_free(void *ptr);
+
+/* Fill a drift_potential for the Bovy composite from physical parameters
+ * (bulge slope alpha, cutoff rc, bulge radial force at r = 1; disk amp, a, b;
+ * halo amp, a).  Host-only arithmetic. */
+int drift_potential_bovy(drift_potential *p, double alpha, double rc, double bulge_force_at_1,
+                         double mn_amp, double mn_a, double mn_b, double nfw_amp,
+                         double nfw_a);
+
+/* Bytes of device workspace drift_integrate needs for this request. */
+int drift_query_workspace(const drift_launch *launch, size_t *bytes);
+
+/* Integrate on the device; all pointers are device pointers.  Replaces the
+ * launch inside backend::launch (src/dispatch/gpu/cuda_oxide.rs:40-73). */
+int drift_integrate(const drift_launch *launch, void *stream);
+
+/* Integrate from host buffers: copies in, launches, copies results out and
+ * synchronises.  Replaces the whole backend::launch
+ * (src/dispatch/gpu/cuda_oxide.rs:9-86), with a library-owned persistent
+ * context instead of one context per call.  Large requests are processed in
+ * particle chunks whose copies overlap the integration of other chunks. */
+int drift_integrate_host(const drift_launch *launch);
+
+/* The reference kernel signatures (kernels/src/lib.rs:143-173, 188-216):
+ * galpy Kepler force, shared output grid, plain schedule, exact precision.
+ * Device pointers; tolerances are natural logarithms. */
+int drift_galpy_dopr54(const double *state0, const double *times, double *state_out, int64_t n,
+                       int64_t nt, double rtol, double atol, double dt_one_init, void *stream);
+int drift_galpy_dop853(const double *state0, const double *times, double *state_out, int64_t n,
+                       int64_t nt, double rtol, double atol, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DRIFT_B200_H */

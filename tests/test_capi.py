@@ -1,0 +1,107 @@
+"""The C ABI library loads, exports every declared symbol and validates its
+arguments on the host (no device work)."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from astrodrift_b200 import capi
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "drift_b200.h"
+
+
+def declared_functions() -> list[str]:
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(drift_\w+)\s*\(", text, re.M)))
+
+
+def test_every_declared_symbol_is_exported():
+    names = declared_functions()
+    assert len(names) >= 11
+    lib = capi.lib()
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert missing == []
+    assert set(names) == set(capi.EXPORTED)
+
+
+def test_abi_version_and_messages():
+    lib = capi.lib()
+    assert lib.drift_abi_version() == 1
+    assert lib.drift_result_string(0) == b"success"
+    assert lib.drift_result_string(1) == b"invalid argument"
+
+
+def test_struct_layout_matches_header(tmp_path):
+    # Compile the header with the C compiler and compare every field offset
+    # with the ctypes mirror used by the tests and the benchmark.
+    import subprocess
+
+    lines = []
+    for struct_name, cls in (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch)):
+        lines.append(f'printf("{struct_name} %zu\\n", sizeof({struct_name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{struct_name}.{field} %zu\\n", offsetof({struct_name}, {field}));')
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "drift_b200.h"\nint main(void){\n'
+                   + "\n".join(lines) + "\nreturn 0;}\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                         check=True).stdout.splitlines())
+    for struct_name, cls in (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch)):
+        assert int(got[struct_name]) == ctypes.sizeof(cls)
+        for field, _ in cls._fields_:
+            assert int(got[f"{struct_name}.{field}"]) == getattr(cls, field).offset, field
+
+
+@pytest.mark.parametrize(
+    "mutate, message",
+    [
+        (lambda L: setattr(L, "n", 0), "n must be >= 1"),
+        (lambda L: setattr(L, "nt", 1), "nt must be"),
+        (lambda L: setattr(L, "method", 7), "unknown method"),
+        (lambda L: setattr(L, "precision", 9), "unknown precision"),
+        (lambda L: setattr(L, "schedule", 9), "unknown schedule"),
+        (lambda L: setattr(L, "block_size", 48), "block_size"),
+        (lambda L: setattr(L.potential, "kind", 11), "unknown potential"),
+        (lambda L: setattr(L, "rtol_ln", float("nan")), "tolerances"),
+        (lambda L: setattr(L, "ts", None), "either ts or t_end"),
+        (lambda L: setattr(L, "y0", None), "y0 is NULL"),
+    ],
+)
+def test_invalid_launches_are_rejected_before_any_device_work(mutate, message):
+    y0 = np.zeros((4, 6))
+    ts = np.linspace(0.0, 1.0, 3)
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 4, 3, rtol=1e-10, atol=1e-10)
+    L.y0 = y0.ctypes.data
+    L.ts = ts.ctypes.data
+    mutate(L)
+    rc = capi.lib().drift_integrate(ctypes.byref(L), None)
+    assert rc == 1
+    assert message in capi.lib().drift_last_error().decode()
+
+
+def test_persistent_schedule_requires_workspace():
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 4, 3, rtol=1e-10, atol=1e-10,
+                         schedule=capi.PERSISTENT)
+    assert capi.query_workspace(L) >= 8
+    L2 = capi.make_launch(capi.DOP853, capi.plummer(), 4, 3, rtol=1e-10, atol=1e-10,
+                          schedule=capi.PLAIN)
+    assert capi.query_workspace(L2) == 0
+
+
+def test_bovy_descriptor_normalises_bulge():
+    from scipy.special import gamma, gammainc
+
+    p = capi.bovy()
+    assert p.kind == capi.POT_BOVY
+    s = 1.5 - 0.5 * 1.8
+    gs = gamma(s)
+    assert abs(p.bulge_gamma_s - gs) < 1e-15 * gs
+    # F_r(1) = -k gamma(s, 1/rc^2) = -0.05
+    assert abs(p.bulge_k * gammainc(s, 1.0 / (1.9 / 8.0) ** 2) * gs - 0.05) < 1e-15
