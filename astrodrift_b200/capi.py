@@ -36,6 +36,7 @@ EXPORTED = (
     "drift_integrate_host",
     "drift_galpy_dopr54",
     "drift_galpy_dop853",
+    "drift_force",
 )
 
 
@@ -108,6 +109,8 @@ def lib() -> ctypes.CDLL:
         L.drift_integrate_host.argtypes = [ctypes.POINTER(DriftLaunch)]
         L.drift_galpy_dopr54.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 3 + [ctypes.c_void_p]
         L.drift_galpy_dop853.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 2 + [ctypes.c_void_p]
+        L.drift_force.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int64, ctypes.c_void_p,
+                                  ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -214,6 +217,12 @@ def query_workspace(L: DriftLaunch) -> int:
 def integrate_device(L: DriftLaunch, stream: int = 0) -> None:
     """drift_integrate on device pointers already stored in ``L``."""
     check(lib().drift_integrate(ctypes.byref(L), ctypes.c_void_p(stream)), "drift_integrate")
+
+
+def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream: int = 0) -> None:
+    """drift_force on device pointers."""
+    check(lib().drift_force(ctypes.byref(pot), n, ctypes.c_void_p(xyz_ptr), ctypes.c_void_p(acc_ptr),
+                            ctypes.c_void_p(stream)), "drift_force")
 
 
 def exported_symbols() -> dict[str, bool]:

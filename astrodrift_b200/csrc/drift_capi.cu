@@ -132,8 +132,10 @@ int validate(const drift_launch *L, bool device_pointers)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown precision");
     if (L->schedule != DRIFT_SCHEDULE_PLAIN && L->schedule != DRIFT_SCHEDULE_PERSISTENT)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown schedule");
-    if (L->block_size != 0 && (L->block_size < 32 || L->block_size > 128 || L->block_size % 32))
-        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "block_size must be 0 or a multiple of 32 in [32, 128]");
+    const int max_block = std::min(drift::max_threads_exact(), drift::max_threads_fma());
+    if (L->block_size != 0 && (L->block_size < 32 || L->block_size > max_block || L->block_size % 32))
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "block_size must be 0 or a multiple of 32 in [32, " + std::to_string(max_block) + "]");
     const int k = L->potential.kind;
     if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown potential kind");
@@ -153,7 +155,11 @@ int validate(const drift_launch *L, bool device_pointers)
     return DRIFT_SUCCESS;
 }
 
-int block_of(const drift_launch *L) { return L->block_size ? L->block_size : DEFAULT_BLOCK; }
+int block_of(const drift_launch *L)
+{
+    if (L->block_size) return L->block_size;
+    return std::min(DEFAULT_BLOCK, std::min(drift::max_threads_exact(), drift::max_threads_fma()));
+}
 
 drift::KernelArgs make_args(const drift_launch *L)
 {
@@ -332,6 +338,25 @@ int drift_integrate(const drift_launch *launch, void *stream)
             return fail(DRIFT_ERROR_WORKSPACE, "persistent schedule needs an 8-byte aligned workspace of at least 8 bytes");
     }
     return launch_device(ctx, launch, launch->workspace, static_cast<cudaStream_t>(stream));
+}
+
+int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
+                void *stream)
+{
+    if (!potential || !xyz || !acc || n < 0)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_force: NULL pointer or negative n");
+    const int k = potential->kind;
+    if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown potential kind");
+    if (n == 0) return DRIFT_SUCCESS;
+    DeviceContext *ctx = nullptr;
+    int rc = current_context(&ctx);
+    if (rc) return rc;
+    int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sm_count * 8);
+    DRIFT_CUDA_TRY(drift::force_exact(*potential, n, xyz, acc, (int)blocks,
+                                      static_cast<cudaStream_t>(stream)),
+                   "force kernel launch");
+    return DRIFT_SUCCESS;
 }
 
 int drift_host_alloc(size_t bytes, void **ptr)

@@ -32,23 +32,27 @@ struct Grid {
     }
 };
 
+__device__ __forceinline__ void store6(double *dst, const double *v)
+{
+    double2 *p = reinterpret_cast<double2 *>(dst);
+    __stcs(p + 0, make_double2(v[0], v[1]));
+    __stcs(p + 1, make_double2(v[2], v[3]));
+    __stcs(p + 2, make_double2(v[4], v[5]));
+}
+
 // Writes one 6-vector of particle `pid` at output slot k of a time-major
-// (nt, n, 6) array with 16-byte vector stores (48 B per sample, aligned).
+// (nt, n, 6) array with 16-byte vector stores (48 B per sample, aligned);
+// the sample at the last output time is also the particle's final state.
 struct TimeMajorOut {
-    double *base;  // NULL: trajectories not requested
+    double *base;     // NULL: trajectories not requested
+    double *y_final;  // NULL: final states not requested
     int64_t n;
     int64_t pid;
-    double last[6];  // most recent sample (the final state once done)
-    __device__ __forceinline__ void write(int32_t k, const double *v)
+    int32_t nt;
+    __device__ __forceinline__ void write(int32_t k, const double *v) const
     {
-#pragma unroll
-        for (int i = 0; i < 6; i++) last[i] = v[i];
-        if (base) {
-            double2 *p = reinterpret_cast<double2 *>(base + ((int64_t)k * n + pid) * 6);
-            __stcs(p + 0, make_double2(v[0], v[1]));
-            __stcs(p + 1, make_double2(v[2], v[3]));
-            __stcs(p + 2, make_double2(v[4], v[5]));
-        }
+        if (base) store6(base + ((int64_t)k * n + pid) * 6, v);
+        if (y_final && k == nt - 1) store6(y_final + pid * 6, v);
     }
 };
 

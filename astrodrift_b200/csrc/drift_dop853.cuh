@@ -11,10 +11,21 @@
 //
 // The state that outlives a step (y, k1 = f(y), h, t, flags) lives in
 // registers; stage vectors are locals of `step` so the compiler can reuse
-// their registers across stages.
+// their registers across stages.  On accept the eight-term partial sums of
+// rcont5..8 must survive the three extra stages; they are parked in this
+// thread's column of a shared-memory tile instead of holding 48 registers
+// through the register-heaviest part of the step.
+//
+// DRIFT_EXACT_ARITH (set by the including translation unit): 1 keeps every
+// division of the reference's error norm; 0 multiplies by one reciprocal per
+// component instead.
 #pragma once
 
 #include "drift_common.cuh"
+
+#ifndef DRIFT_EXACT_ARITH
+#define DRIFT_EXACT_ARITH 1
+#endif
 
 namespace drift {
 namespace dop853c {
@@ -170,6 +181,7 @@ constexpr double FACC2 = 1.0 / 6.0;
 // step h = 1e3 * UROUND forever in that situation.
 constexpr int DOP853_NONFINITE_LIMIT = 64;
 
+
 template <class Pot>
 struct Dop853Lane {
     double y[6];   // current solution (y0 in the reference)
@@ -239,11 +251,13 @@ struct Dop853Lane {
     }
 
     // One step attempt (dop853.rs:425-782).  Returns true when accepted.
+    // `park` is this thread's column of a [24][blockDim.x] shared tile.
     template <class Out>
     __device__ __forceinline__ bool step(const Pot &pot, const Grid &grid, double rtol,
-                                         double atol, Out &out)
+                                         double atol, Out &out, volatile double *park)
     {
         using namespace dop853c;
+        const int RCONT_STRIDE = blockDim.x;
         h = pos_neg * c_max(fabs(h), 1e3 * UROUND);
         double yy1[6], k2[6], k3[6], k4[6], k5[6], k6[6], k7[6], k8[6], k9[6], k10[6];
 
@@ -308,12 +322,23 @@ struct Dop853Lane {
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             double sk = atol + rtol * c_max(fabs(y[i]), fabs(k5[i]));
+#if !DRIFT_EXACT_ARITH
+            double inv_sk = 1.0 / sk;
+#endif
             double erri = k4[i] - BHH1 * k1[i] - BHH2 * k9[i] - BHH3 * k3[i];
+#if DRIFT_EXACT_ARITH
             double sqr = erri / sk;
+#else
+            double sqr = erri * inv_sk;
+#endif
             err2 += sqr * sqr;
             erri = ER1 * k1[i] + ER6 * k6[i] + ER7 * k7[i] + ER8 * k8[i] + ER9 * k9[i] +
                    ER10 * k10[i] + ER11 * k2[i] + ER12 * k3[i];
+#if DRIFT_EXACT_ARITH
             sqr = erri / sk;
+#else
+            sqr = erri * inv_sk;
+#endif
             err += sqr * sqr;
         }
         double deno = err + 0.01 * err2;
@@ -330,17 +355,20 @@ struct Dop853Lane {
             nonfinite_run = 0;
             rhs(pot, k5, k4);  // FSAL: k4 = f(t_new, y_new)
 
-            double r5[6], r6[6], r7[6], r8[6];
 #pragma unroll
             for (int i = 0; i < 6; i++) {
-                r5[i] = D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
-                        D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
-                r6[i] = D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
-                        D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
-                r7[i] = D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
-                        D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
-                r8[i] = D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
-                        D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
+                park[(0 * 6 + i) * RCONT_STRIDE] =
+                    D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
+                    D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
+                park[(1 * 6 + i) * RCONT_STRIDE] =
+                    D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
+                    D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
+                park[(2 * 6 + i) * RCONT_STRIDE] =
+                    D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
+                    D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
+                park[(3 * 6 + i) * RCONT_STRIDE] =
+                    D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
+                    D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
             }
 #pragma unroll
             for (int i = 0; i < 6; i++)
@@ -363,13 +391,17 @@ struct Dop853Lane {
 
             // rcont1..4 (dop853.rs:636-642) need only y, y_new, k1 and k4,
             // so they are formed here, after the extra stages.
-            double r1[6], r2[6], r3[6], r4[6];
+            double r1[6], r2[6], r3[6], r4[6], r5[6], r6[6], r7[6], r8[6];
 #pragma unroll
             for (int i = 0; i < 6; i++) {
-                r5[i] = h * (r5[i] + D413 * k4[i] + D414 * k10[i] + D415 * k2[i] + D416 * k3[i]);
-                r6[i] = h * (r6[i] + D513 * k4[i] + D514 * k10[i] + D515 * k2[i] + D516 * k3[i]);
-                r7[i] = h * (r7[i] + D613 * k4[i] + D614 * k10[i] + D615 * k2[i] + D616 * k3[i]);
-                r8[i] = h * (r8[i] + D713 * k4[i] + D714 * k10[i] + D715 * k2[i] + D716 * k3[i]);
+                r5[i] = h * (park[(0 * 6 + i) * RCONT_STRIDE] + D413 * k4[i] + D414 * k10[i] +
+                             D415 * k2[i] + D416 * k3[i]);
+                r6[i] = h * (park[(1 * 6 + i) * RCONT_STRIDE] + D513 * k4[i] + D514 * k10[i] +
+                             D515 * k2[i] + D516 * k3[i]);
+                r7[i] = h * (park[(2 * 6 + i) * RCONT_STRIDE] + D613 * k4[i] + D614 * k10[i] +
+                             D615 * k2[i] + D616 * k3[i]);
+                r8[i] = h * (park[(3 * 6 + i) * RCONT_STRIDE] + D713 * k4[i] + D714 * k10[i] +
+                             D715 * k2[i] + D716 * k3[i]);
                 r1[i] = y[i];
                 double ydiff = k5[i] - y[i];
                 r2[i] = ydiff;

@@ -39,9 +39,26 @@ __device__ __forceinline__ int64_t claim_particle(unsigned long long *cursor)
     return (int64_t)(base + (unsigned long long)__popc(below));
 }
 
+// Launch bounds of the integration kernels: at most DRIFT_MAX_THREADS
+// threads per block, and registers allocated so that DRIFT_MIN_BLOCKS_PER_SM
+// such blocks can be resident on one SM.
+#ifndef DRIFT_MAX_THREADS
+#define DRIFT_MAX_THREADS 128
+#endif
+#ifndef DRIFT_MIN_BLOCKS_PER_SM
+#define DRIFT_MIN_BLOCKS_PER_SM 3
+#endif
+
+// Dynamic shared memory per block: the DOP853 rcont parking tile,
+// 24 doubles per thread, column-major by thread.
+__host__ __device__ constexpr size_t park_bytes(int block) { return 24 * sizeof(double) * block; }
+
 template <int METHOD, class Pot>
-__global__ void __launch_bounds__(128) integrate_kernel(KernelArgs a)
+__global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
+    integrate_kernel(KernelArgs a)
 {
+    extern __shared__ double rcont_park[];
+    volatile double *park = rcont_park + threadIdx.x;
     const Pot pot(a.potential);
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t deadline = a.timeout_ns ? global_timer_ns() + a.timeout_ns : 0;
@@ -50,7 +67,9 @@ __global__ void __launch_bounds__(128) integrate_kernel(KernelArgs a)
     Dopr54Lane<Pot> l54;
     TimeMajorOut out;
     out.base = a.out;
+    out.y_final = a.y_final;
     out.n = a.n;
+    out.nt = a.nt;
     Grid grid;
     grid.ts = a.ts;
     grid.t0 = a.t0;
@@ -102,47 +121,54 @@ __global__ void __launch_bounds__(128) integrate_kernel(KernelArgs a)
         if (a.err_code) a.err_code[pid] = code;
         if (a.n_accepted) a.n_accepted[pid] = nacc;
         if (a.n_rejected) a.n_rejected[pid] = nrej;
-        if (a.y_final) {
-            double2 *dst = reinterpret_cast<double2 *>(a.y_final + pid * 6);
-            dst[0] = make_double2(out.last[0], out.last[1]);
-            dst[1] = make_double2(out.last[2], out.last[3]);
-            dst[2] = make_double2(out.last[4], out.last[5]);
-        }
         active = false;
     };
 
+    // Warp-uniform control: every lane of the warp stays in the loop until
+    // no lane has work, and the vote at the top of each iteration makes the
+    // lanes reconverge before the next step, so one step instruction stream
+    // serves all particles of the warp.
+    bool exhausted = false;  // no further particle for this lane
     if (!a.persistent) {
-        if (gtid >= a.n) return;
-        start(gtid);
+        if (gtid < a.n)
+            start(gtid);
+        else
+            exhausted = true;
     }
-
     while (true) {
-        if (!active) {
-            if (!a.persistent) break;
+        if (a.persistent && !active && !exhausted) {
             int64_t p = claim_particle(a.cursor);
-            if (p >= a.n) break;
-            start(p);
+            if (p < a.n)
+                start(p);
+            else
+                exhausted = true;
         }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
         bool done = (METHOD == DRIFT_DOP853) ? l853.done : l54.done;
         if (done) {
             finish(DRIFT_PARTICLE_OK);
+            if (!a.persistent) exhausted = true;
             continue;
         }
         if (attempts >= a.max_steps) {
             finish(DRIFT_PARTICLE_MAX_STEPS);
+            if (!a.persistent) exhausted = true;
             continue;
         }
         if (deadline != 0 && (attempts & 63) == 0 && global_timer_ns() > deadline) {
             finish(DRIFT_PARTICLE_TIMEOUT);
+            if (!a.persistent) exhausted = true;
             continue;
         }
         attempts++;
         bool accepted;
         if (METHOD == DRIFT_DOP853) {
-            accepted = l853.step(pot, grid, a.rtol, a.atol, out);
+            accepted = l853.step(pot, grid, a.rtol, a.atol, out, park);
             if (!accepted && l853.nonfinite_run >= DOP853_NONFINITE_LIMIT) {
                 nrej++;
                 finish(DRIFT_PARTICLE_NONFINITE);
+                if (!a.persistent) exhausted = true;
                 continue;
             }
         } else {
@@ -155,6 +181,36 @@ __global__ void __launch_bounds__(128) integrate_kernel(KernelArgs a)
     }
 }
 
+template <class Pot>
+__global__ void __launch_bounds__(256) force_kernel(drift_potential p, int64_t n, const double *xyz,
+                                                    double *acc)
+{
+    const Pot pot(p);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double ax, ay, az;
+        pot.force(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], ax, ay, az);
+        acc[3 * i] = ax;
+        acc[3 * i + 1] = ay;
+        acc[3 * i + 2] = az;
+    }
+}
+
+inline cudaError_t force_impl(const drift_potential &p, int64_t n, const double *xyz, double *acc,
+                              int grid, cudaStream_t stream)
+{
+    switch (p.kind) {
+    case DRIFT_POT_KEPLER: force_kernel<KeplerGalpy><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
+    case DRIFT_POT_PLUMMER: force_kernel<Plummer><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
+    case DRIFT_POT_BOVY: force_kernel<Bovy><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
+    case DRIFT_POT_KEPLER_CARTESIAN:
+        force_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(p, n, xyz, acc);
+        break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
 // Host-side launcher for this precision unit.
 inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int block,
                                cudaStream_t stream)
@@ -162,7 +218,7 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
     const int kind = a.potential.kind;
 #define DRIFT_LAUNCH(M, P)                                                       \
     do {                                                                         \
-        integrate_kernel<M, P><<<grid, block, 0, stream>>>(a);                   \
+        integrate_kernel<M, P><<<grid, block, M == DRIFT_DOP853 ? park_bytes(block) : 0, stream>>>(a); \
         return cudaGetLastError();                                               \
     } while (0)
 #define DRIFT_POT_SWITCH(M)                                                      \
@@ -182,11 +238,13 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
 #undef DRIFT_LAUNCH
 }
 
+inline int max_threads_impl() { return DRIFT_MAX_THREADS; }
+
 inline cudaError_t occupancy_impl(int method, int kind, int block, int *blocks_per_sm)
 {
 #define DRIFT_OCC(M, P)                                                                     \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm,                     \
-                                                         integrate_kernel<M, P>, block, 0)
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                   \
+        blocks_per_sm, integrate_kernel<M, P>, block, M == DRIFT_DOP853 ? park_bytes(block) : 0)
 #define DRIFT_OCC_SWITCH(M)                                                     \
     switch (kind) {                                                             \
     case DRIFT_POT_KEPLER: DRIFT_OCC(M, KeplerGalpy);                           \

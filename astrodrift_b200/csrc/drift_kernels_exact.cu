@@ -1,5 +1,6 @@
 // Integration kernels without multiply-add contraction (compiled -fmad=false):
 // the stage arithmetic rounds exactly as the reference's Rust code does.
+#define DRIFT_EXACT_ARITH 1
 #define DRIFT_PRECISION_NS exact
 #include "drift_kernels.cuh"
 
@@ -9,6 +10,12 @@ cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
 {
     return exact::launch_impl(a, method, grid, block, stream);
 }
+cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
+                        int grid, cudaStream_t stream)
+{
+    return exact::force_impl(p, n, xyz, acc, grid, stream);
+}
+int max_threads_exact() { return exact::max_threads_impl(); }
 cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)
 {
     return exact::occupancy_impl(method, kind, block, blocks_per_sm);

@@ -1,4 +1,5 @@
 // Integration kernels with multiply-add contraction (compiled -fmad=true).
+#define DRIFT_EXACT_ARITH 0
 #define DRIFT_PRECISION_NS fma_mode
 #include "drift_kernels.cuh"
 
@@ -8,6 +9,7 @@ cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
 {
     return fma_mode::launch_impl(a, method, grid, block, stream);
 }
+int max_threads_fma() { return fma_mode::max_threads_impl(); }
 cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm)
 {
     return fma_mode::occupancy_impl(method, kind, block, blocks_per_sm);

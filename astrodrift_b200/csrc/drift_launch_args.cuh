@@ -39,6 +39,10 @@ cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
 cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
                        cudaStream_t stream);
 cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm);
+int max_threads_exact();
+int max_threads_fma();
+cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
+                        int grid, cudaStream_t stream);
 cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm);
 
 }  // namespace drift

@@ -4,7 +4,7 @@
 // the DOP853 controller and pow(x, 1.5) in the Miyamoto-Nagai disk, all
 // through glibc's pow, which returns the correctly rounded result except in
 // rare near-halfway cases.  These routines compute the same powers from IEEE
-// sqrt and division plus one Newton correction carried in double-double
+// sqrt / rsqrt and division plus one Newton correction carried in double-double
 // (two-term) arithmetic, so the result is the correctly rounded value unless
 // the exact power lies within about 2^-50 ulp of a rounding boundary.  They
 // are written from the algebra below; no vendor math code is reproduced.
@@ -12,7 +12,11 @@
 //   x^(3/2):  s = RN(sqrt x), e = x - s^2 exactly (one fma), so
 //             sqrt x = s + e/(2s) + O(e^2) and x^(3/2) = x s + x e/(2s)
 //             = x s + e s / 2 (1 + O(2^-52)).
-//   x^(-3/2): r = 1 / x^(3/2) refined as r = rh (1 + (1 - rh (ph + pl))).
+//   x^(-3/2): r0 = y^3 with y a Newton-refined rsqrt estimate is within a
+//             few ulps; one Newton step on
+//             r^-2 = x^3 gives r = r0 (1 + delta / 2) with
+//             delta = 1 - r0^2 x^3 formed in double-double (x^3 and r0^2
+//             as exact products), leaving an error of order delta^2.
 //   x^(1/8):  y0 = sqrt(sqrt(sqrt x)) is within about one ulp; one Newton
 //             step on y^8 = x with y0^8 formed in double-double gives
 //             y = y0 (1 - (y0^8 - x) / (8 x)).
@@ -64,20 +68,33 @@ __device__ __forceinline__ double pow_1p5(double x)
     return scalbn(hi + lo, 3 * k);
 }
 
+// Valid for x in [1e-90, 1e90] (x^3 and its low part stay normal).
 __device__ __forceinline__ double pow_m1p5_core(double x)
 {
-    double ph, pl;
-    pow_1p5_dd(x, ph, pl);
-    double rh = 1.0 / ph;
-    double eps = fma(-rh, ph, 1.0) - rh * pl;
-    return fma(rh, eps, rh);
+    // Hardware estimate (PTX rsqrt.approx.f64, about 2^-23 relative error on
+    // normal inputs) refined by two Newton steps y <- y (3 - x y^2) / 2 to a
+    // few ulps; the double-double step below then rounds correctly.
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    y = y * fma(-0.5 * x, y * y, 1.5);
+    y = y * fma(-0.5 * x, y * y, 1.5);
+    double r0 = y * y * y;
+    double a, al, b, bl, c, cl, p, pl;
+    two_prod(x, x, a, al);      // x^2
+    two_prod(a, x, b, bl);      // x^3 = b + bl
+    bl = fma(al, x, bl);
+    two_prod(r0, r0, c, cl);    // r0^2 = c + cl
+    two_prod(c, b, p, pl);      // r0^2 x^3 = p + pl
+    pl = fma(c, bl, fma(cl, b, pl));
+    double delta = (1.0 - p) - pl;
+    return fma(r0, 0.5 * delta, r0);
 }
 
 // x^(-3/2), rounded to nearest (pow(x, -1.5) semantics, including the
 // special values: +-0 -> +inf, +inf -> +0, x < 0 -> NaN).
 __device__ __forceinline__ double pow_m1p5(double x)
 {
-    if (in_fast_range(x)) return pow_m1p5_core(x);
+    if (x > 1e-90 && x < 1e90) return pow_m1p5_core(x);
     if (x == 0.0) return __longlong_as_double(0x7ff0000000000000LL);  // +inf
     if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);
     if (isinf(x)) return 0.0;

@@ -17,12 +17,21 @@
 #include "drift_math.cuh"
 #include "drift_b200.h"
 
+// DRIFT_FORCE_NOINLINE: keep one out-of-line copy of each force body instead
+// of inlining it at every stage (the integrators evaluate it up to 17 times
+// per step, and the inlined copies compete for instruction cache).
+#ifdef DRIFT_FORCE_NOINLINE
+#define DRIFT_FORCE_FN __noinline__
+#else
+#define DRIFT_FORCE_FN __forceinline__
+#endif
+
 namespace drift {
 
 struct KeplerGalpy {
     double amp;
     __host__ __device__ explicit KeplerGalpy(const drift_potential &p) : amp(p.amp) {}
-    __device__ __forceinline__ void force(double x, double y, double z, double &ax, double &ay,
+    __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
         double cylindrical_radius = sqrt(x * x + y * y);
@@ -43,7 +52,7 @@ struct KeplerGalpy {
 struct KeplerCartesian {
     double amp;
     __host__ __device__ explicit KeplerCartesian(const drift_potential &p) : amp(p.amp) {}
-    __device__ __forceinline__ void force(double x, double y, double z, double &ax, double &ay,
+    __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
         double r2 = x * x + y * y + z * z;
@@ -59,7 +68,7 @@ struct KeplerCartesian {
 struct Plummer {
     double amp, b2;
     __host__ __device__ explicit Plummer(const drift_potential &p) : amp(p.amp), b2(p.b * p.b) {}
-    __device__ __forceinline__ void force(double x, double y, double z, double &ax, double &ay,
+    __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
         double r2 = x * x + y * y + z * z;
@@ -122,7 +131,7 @@ struct Bovy {
     {
     }
 
-    __device__ __forceinline__ void force(double x, double y, double z, double &ax, double &ay,
+    __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
         // bulge

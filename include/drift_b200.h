@@ -170,6 +170,13 @@ int drift_integrate(const drift_launch *launch, void *stream);
  * particle chunks whose copies overlap the integration of other chunks. */
 int drift_integrate_host(const drift_launch *launch);
 
+/* Acceleration of the potential at n positions: xyz (n, 3) -> acc (n, 3),
+ * device pointers, the same force code the integrators inline (rounded
+ * without multiply-add contraction).  The reference exposes the force only
+ * through its Potential trait (shared/src/potential.rs:41-44). */
+int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
+                void *stream);
+
 /* The reference kernel signatures (kernels/src/lib.rs:143-173, 188-216):
  * galpy Kepler force, shared output grid, plain schedule, exact precision.
  * Device pointers; tolerances are natural logarithms. */
