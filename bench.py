@@ -209,8 +209,12 @@ def main() -> None:
     ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
-    ap.add_argument("--cpu-sample", type=int, default=4096)
+    ap.add_argument("--cpu-sample", type=int, default=262144)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-peak", action="store_true", help="skip the FP64 peak probe (profiling runs)")
+    ap.add_argument("--particles", type=int, default=N_PARTICLES,
+                    help="particles per GPU (default: the workload's 2^20; smaller for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
@@ -233,7 +237,7 @@ def main() -> None:
                                 device_id=torch.device(f"cuda:{local}"))
     dev = torch.device(f"cuda:{local}")
 
-    y0 = plummer_sphere(N_PARTICLES, seed=2 + rank)
+    y0 = plummer_sphere(N_PARTICLES, seed=2 + rank)[: args.particles]
     ts = np.linspace(*TS[:2], TS[2])
     n, nt = len(y0), len(ts)
     precision = capi.EXACT if args.precision == "exact" else capi.FMA
@@ -302,41 +306,46 @@ def main() -> None:
     # --- end to end through the host entry point with pinned buffers --------
     import ctypes
 
-    lib = capi.lib()
-    h_y0 = ctypes.c_void_p()
-    h_out = ctypes.c_void_p()
+    if args.no_e2e:
+        args.e2e_steps = 0
+
     out_bytes = nt * n * 6 * 8
-    capi.check(lib.drift_host_alloc(y0.nbytes, ctypes.byref(h_y0)), "drift_host_alloc")
-    capi.check(lib.drift_host_alloc(out_bytes, ctypes.byref(h_out)), "drift_host_alloc")
-    y0_pinned = np.ctypeslib.as_array((ctypes.c_double * (n * 6)).from_address(h_y0.value)).reshape(n, 6)
-    y0_pinned[:] = y0
-    out_pinned = np.ctypeslib.as_array((ctypes.c_double * (nt * n * 6)).from_address(h_out.value)).reshape(nt, n, 6)
-    h_acc = np.empty(n, np.uint32)
+    e2e_value, e2e_elapsed, e2e_ok = None, 0.0, None
+    if args.e2e_steps > 0:
+        lib = capi.lib()
+        h_y0, h_out = ctypes.c_void_p(), ctypes.c_void_p()
+        capi.check(lib.drift_host_alloc(y0.nbytes, ctypes.byref(h_y0)), "drift_host_alloc")
+        capi.check(lib.drift_host_alloc(out_bytes, ctypes.byref(h_out)), "drift_host_alloc")
+        y0_pinned = np.ctypeslib.as_array(
+            (ctypes.c_double * (n * 6)).from_address(h_y0.value)).reshape(n, 6)
+        y0_pinned[:] = y0
+        out_pinned = np.ctypeslib.as_array(
+            (ctypes.c_double * (nt * n * 6)).from_address(h_out.value)).reshape(nt, n, 6)
 
-    def e2e_step():
-        capi.integrate_host(capi.DOP853, capi.plummer(1.0, 1.0), y0_pinned, ts=ts, rtol=RTOL,
-                            atol=ATOL, precision=precision, schedule=schedule,
-                            block_size=args.block, out=out_pinned)
+        def e2e_step():
+            capi.integrate_host(capi.DOP853, capi.plummer(1.0, 1.0), y0_pinned, ts=ts, rtol=RTOL,
+                                atol=ATOL, precision=precision, schedule=schedule,
+                                block_size=args.block, out=out_pinned)
 
-    e2e_step()
-    if dist:
-        dist.barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
         e2e_step()
-    e2e_elapsed = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
-    e2e_value = accepted_all * args.e2e_steps / e2e_elapsed
-    e2e_ok = np.array_equal(out_pinned[-1], out_d[-1].cpu().numpy())
-    lib.drift_host_free(h_y0)
-    lib.drift_host_free(h_out)
-    del y0_pinned, out_pinned, h_acc
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            e2e_step()
+        e2e_elapsed = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_elapsed = float(t.item())
+        e2e_value = accepted_all * args.e2e_steps / e2e_elapsed
+        e2e_ok = bool(np.array_equal(out_pinned[-1], out_d[-1].cpu().numpy()))
+        del y0_pinned, out_pinned
+        lib.drift_host_free(h_y0)
+        lib.drift_host_free(h_out)
 
     if rank == 0:
-        fp64_peak = fp64_peak_tflops(torch)
+        fp64_peak = float("nan") if args.no_peak else fp64_peak_tflops(torch)
         hbm_peak, hbm_src = measured_hbm_gbs()
         mean_launch = statistics.mean(launch_s)
         samples = n * (nt - 1)
@@ -363,7 +372,8 @@ def main() -> None:
             "vs_baseline": None,
             "dtype": "f64",
             "data": "synthetic (seeded isotropic Plummer DF, amp=1, b=1)",
-            "config": {"workload": WORKLOAD, "particles_per_gpu": n, "ts": list(TS),
+            "config": {"workload": WORKLOAD if n == N_PARTICLES else f"{WORKLOAD} (subset of {n})",
+                       "particles_per_gpu": n, "ts": list(TS),
                        "rtol": RTOL, "atol": ATOL, "method": "DOP853",
                        "potential": "plummer(amp=1, b=1)", "precision": args.precision,
                        "schedule": args.schedule,
@@ -387,8 +397,8 @@ def main() -> None:
             "e2e": {"value": e2e_value, "unit": "accepted steps/s",
                     "h2d_bytes_per_step": int(y0.nbytes + ts.nbytes),
                     "d2h_bytes_per_step": int(out_bytes + n * (48 + 1 + 4 + 4 + 4)),
-                    "ms_per_step": 1e3 * e2e_elapsed / args.e2e_steps,
-                    "matches_device_path": bool(e2e_ok)},
+                    "ms_per_step": 1e3 * e2e_elapsed / max(args.e2e_steps, 1),
+                    "matches_device_path": e2e_ok},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

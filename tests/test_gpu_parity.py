@@ -126,13 +126,19 @@ def test_potential_batches_match_oracle(oracle, cuda_device, pname, method, prec
     g = np.load(GOLDEN / "potential_batches.npz")
     m, om = METHODS[method]
     y0, ts = g[f"{pname}_y0"], g["ts"]
-    got = capi.integrate_host(m, capi_pot(pname), y0, ts=ts, rtol=1e-10, atol=1e-10,
+    rtol = 1e-10
+    got = capi.integrate_host(m, capi_pot(pname), y0, ts=ts, rtol=rtol, atol=rtol,
                               precision=precision, schedule=schedule)
+    # Exact mode rounds every stage as the reference does: 1e-9.  FMA mode
+    # takes a different (equally accurate) rounding path, so its step
+    # sequence drifts and the two integrations differ at the scale of the
+    # integration error: 100 rtol.
+    tol = REL_TOL if precision == capi.EXACT else max(REL_TOL, 100 * rtol)
     assert (got["status"] == 0).all()
-    assert rel_err(got["out"][-1], g[f"{pname}_{method}_final"]) < REL_TOL
-    assert rel_err(got["out"][20], g[f"{pname}_{method}_mid"]) < REL_TOL
-    ref = oracle.integrate_batch(om, oracle_pot(oracle, pname), y0, ts=ts, rtol=1e-10, atol=1e-10)
-    assert rel_err(got["out"], ref["out"]) < REL_TOL
+    assert rel_err(got["out"][-1], g[f"{pname}_{method}_final"]) < tol
+    assert rel_err(got["out"][20], g[f"{pname}_{method}_mid"]) < tol
+    ref = oracle.integrate_batch(om, oracle_pot(oracle, pname), y0, ts=ts, rtol=rtol, atol=rtol)
+    assert rel_err(got["out"], ref["out"]) < tol
     np.testing.assert_array_equal(got["y_final"], got["out"][-1])
     same = (got["accepted"].astype(np.int64) == g[f"{pname}_{method}_accepted"]).mean()
     assert same >= (0.95 if precision == capi.EXACT else 0.85), same
