@@ -37,6 +37,7 @@ EXPORTED = (
     "drift_galpy_dopr54",
     "drift_galpy_dop853",
     "drift_force",
+    "drift_integrate_noalloc",
 )
 
 
@@ -111,6 +112,7 @@ def lib() -> ctypes.CDLL:
         L.drift_galpy_dop853.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 2 + [ctypes.c_void_p]
         L.drift_force.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int64, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p]
+        L.drift_integrate_noalloc.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -217,6 +219,12 @@ def query_workspace(L: DriftLaunch) -> int:
 def integrate_device(L: DriftLaunch, stream: int = 0) -> None:
     """drift_integrate on device pointers already stored in ``L``."""
     check(lib().drift_integrate(ctypes.byref(L), ctypes.c_void_p(stream)), "drift_integrate")
+
+
+def integrate_device_noalloc(L: DriftLaunch, stream: int = 0) -> None:
+    """drift_integrate_noalloc on device pointers already stored in ``L`` (no workspace)."""
+    check(lib().drift_integrate_noalloc(ctypes.byref(L), ctypes.c_void_p(stream)),
+          "drift_integrate_noalloc")
 
 
 def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream: int = 0) -> None:

@@ -340,6 +340,91 @@ int drift_integrate(const drift_launch *launch, void *stream)
     return launch_device(ctx, launch, launch->workspace, static_cast<cudaStream_t>(stream));
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// drift_integrate_noalloc: drift_integrate for callers that cannot allocate
+// device memory.  Its only scratch -- the persistent schedule's claim cursor
+// -- lives in the fixed array below, which the module carries for as long as
+// the library is loaded on a device.
+// ---------------------------------------------------------------------------
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[DRIFT_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device.  In host code the array's name is only a host-side stand-in;
+// kernels must receive this address instead.
+int noalloc_scratch(int device, void **out)
+{
+    if (device < 0 || device >= NOALLOC_MAX_DEVICES)
+        return fail(DRIFT_ERROR_NO_DEVICE, "drift_integrate_noalloc: device index out of range");
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+        g_noalloc_ptr[device] = ptr;
+    }
+    *out = g_noalloc_ptr[device];
+    return DRIFT_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int drift_integrate_noalloc(const drift_launch *launch, void *stream)
+{
+    int rc = validate(launch, true);
+    if (rc) return rc;
+    size_t need = 0;
+    rc = drift_query_workspace(launch, &need);
+    if (rc) return rc;
+    if (need > DRIFT_NOALLOC_SCRATCH_BYTES)
+        return fail(DRIFT_ERROR_WORKSPACE,
+                    "drift_integrate_noalloc: this request needs " + std::to_string(need) +
+                        " bytes of scratch but the library's fixed scratch holds " +
+                        std::to_string((size_t)DRIFT_NOALLOC_SCRATCH_BYTES) +
+                        "; use drift_integrate with a caller-provided workspace");
+    int device = -1;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(DRIFT_ERROR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
+    void *scratch = nullptr;
+    rc = noalloc_scratch(device, &scratch);
+    if (rc) return rc;
+    int sm_count = 0;
+    DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device),
+                   "cudaDeviceGetAttribute");
+
+    drift::KernelArgs a = make_args(launch);
+    const int block = block_of(launch);
+    int64_t blocks = (launch->n + block - 1) / block;
+    if (a.persistent) {
+        int per_sm = 0;
+        e = launch->precision == DRIFT_PRECISION_EXACT
+                ? drift::occupancy_exact(launch->method, launch->potential.kind, block, &per_sm)
+                : drift::occupancy_fma(launch->method, launch->potential.kind, block, &per_sm);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
+        blocks = std::min(blocks, (int64_t)std::max(per_sm, 1) * sm_count);
+    }
+    if (blocks > INT32_MAX) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "too many particles for one launch");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (a.persistent) {
+        // The array keeps the previous call's contents; the cursor must start at 0.
+        a.cursor = static_cast<unsigned long long *>(scratch);
+        DRIFT_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s), "cudaMemsetAsync");
+    }
+    DRIFT_CUDA_TRY(launch_args(a, launch->method, launch->precision, (int)blocks, block, s),
+                   "kernel launch");
+    return DRIFT_SUCCESS;
+}
+
+extern "C" {
+
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream)
 {

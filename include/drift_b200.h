@@ -177,6 +177,36 @@ int drift_integrate_host(const drift_launch *launch);
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream);
 
+/* Bytes of device scratch that drift_integrate_noalloc owns (per device). */
+#define DRIFT_NOALLOC_SCRATCH_BYTES 4096
+
+/* drift_integrate for callers that cannot allocate device memory.
+ *
+ * No counterpart in the reference (its launch path allocates and frees
+ * buffers on every call).  Some callers of this library own every byte of
+ * device memory themselves and cannot call cudaMalloc: a host application
+ * whose memory pool has reserved the GPU in advance, a real-time loop where
+ * an allocation's implicit synchronisation would stall the pipeline, or a
+ * plugin running inside another runtime that forbids allocation.  For them
+ * this entry point takes the same request as drift_integrate, with device
+ * pointers for every input and output, and allocates nothing: the only
+ * scratch the kernels need (the persistent schedule's claim cursor) lives in
+ * a fixed DRIFT_NOALLOC_SCRATCH_BYTES array inside the library, which every
+ * GPU that loads the library holds until the process exits.
+ * launch->workspace is ignored.
+ *
+ * Limits and rules:
+ *  - a request whose drift_query_workspace size exceeds
+ *    DRIFT_NOALLOC_SCRATCH_BYTES is rejected with DRIFT_ERROR_WORKSPACE;
+ *  - the first call on a device looks up the array's device address for
+ *    that device (with that device current); make that first call before
+ *    any CUDA stream capture;
+ *  - every call shares the one array and clears the part that must start
+ *    at zero before its launch, so calls whose kernels overlap on the GPU
+ *    (different streams, or different host threads) race with each other:
+ *    order them on one stream or serialise them. */
+int drift_integrate_noalloc(const drift_launch *launch, void *stream);
+
 /* The reference kernel signatures (kernels/src/lib.rs:143-173, 188-216):
  * galpy Kepler force, shared output grid, plain schedule, exact precision.
  * Device pointers; tolerances are natural logarithms. */
