@@ -139,6 +139,21 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
     const double rtol_ln = std::log(config.tolerance.rtol);
     const double atol_ln = std::log(config.tolerance.atol);
 
+    // Every stage's force source is checked before any device work starts.
+    std::vector<const Recipe *> stage_force;
+    for (size_t k = 0; k < plan.stages.size(); k++) {
+        const Stage &stage = plan.stages[k];
+        std::vector<const Recipe *> backgrounds;
+        for (size_t i = 0; i < stage.recipes.size(); i++)
+            if (stage.recipe_is_background[i]) backgrounds.push_back(&stage.recipes[i]);
+        if (backgrounds.size() != 1)
+            raise_not_implemented(fmt(
+                "stage %zu requires %zu stationary background potentials; the GPU path integrates "
+                "exactly one (potentials attached to particle groups are not yet force sources)",
+                k + 1, backgrounds.size()));
+        stage_force.push_back(backgrounds[0]);
+    }
+
     std::vector<py::array_t<double>> results;
     int64_t total_particles = 0;
     static bool backend_announced = false;
@@ -149,15 +164,7 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         const int64_t n = *c.num_particles;
         total_particles += n;
         DRIFT_LOG(LOG_GPU, LOG_DEBUG, fmt("stage %d: dispatching %lld particles to the GPU", stage_no, (long long)n));
-
-        std::vector<const Recipe *> backgrounds;
-        for (size_t i = 0; i < stage.recipes.size(); i++)
-            if (stage.recipe_is_background[i]) backgrounds.push_back(&stage.recipes[i]);
-        if (backgrounds.size() != 1)
-            raise_not_implemented(fmt(
-                "stage %d requires %zu stationary background potentials; the GPU path integrates "
-                "exactly one (potentials attached to particle groups are not yet force sources)",
-                stage_no, backgrounds.size()));
+        const Recipe *force_source = stage_force[stage_no - 1];
 
         drift_launch L;
         std::memset(&L, 0, sizeof(L));
@@ -165,7 +172,7 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         L.precision = config.precision == Precision::EXACT ? DRIFT_PRECISION_EXACT : DRIFT_PRECISION_FMA;
         L.schedule = config.schedule == Schedule::PLAIN ? DRIFT_SCHEDULE_PLAIN : DRIFT_SCHEDULE_PERSISTENT;
         L.block_size = config.block_size;
-        L.potential = potential_of(*backgrounds[0]);
+        L.potential = potential_of(*force_source);
         L.n = n;
         L.y0 = c.state->data();
         L.nt = ts.steps;
