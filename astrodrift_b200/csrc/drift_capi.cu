@@ -18,7 +18,16 @@
 #include <vector>
 
 #include "drift_b200.h"
+#include "drift_bulge_table.h"
 #include "drift_launch_args.cuh"
+
+namespace drift {
+void fill_bulge_table(double s, BulgeTable *t)
+{
+    fill_bulge_table_impl(s, t->c, BULGE_SERIES_DEG, BULGE_PIECES, BULGE_PIECE_DEG,
+                          BULGE_FIRST_CENTRE);
+}
+}  // namespace drift
 
 namespace {
 
@@ -189,6 +198,8 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.n_accepted = L->n_accepted;
     a.n_rejected = L->n_rejected;
     a.potential = L->potential;
+    if (L->potential.kind == DRIFT_POT_BOVY)
+        drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
     return a;
 }
 
@@ -438,7 +449,10 @@ int drift_force(const drift_potential *potential, int64_t n, const double *xyz, 
     int rc = current_context(&ctx);
     if (rc) return rc;
     int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sm_count * 8);
-    DRIFT_CUDA_TRY(drift::force_exact(*potential, n, xyz, acc, (int)blocks,
+    drift::BulgeTable table;
+    std::memset(&table, 0, sizeof(table));
+    if (k == DRIFT_POT_BOVY) drift::fill_bulge_table(1.5 - 0.5 * potential->bulge_alpha, &table);
+    DRIFT_CUDA_TRY(drift::force_exact(*potential, n, xyz, acc, table, (int)blocks,
                                       static_cast<cudaStream_t>(stream)),
                    "force kernel launch");
     return DRIFT_SUCCESS;

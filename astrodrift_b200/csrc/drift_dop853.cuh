@@ -323,7 +323,7 @@ struct Dop853Lane {
         for (int i = 0; i < 6; i++) {
             double sk = atol + rtol * c_max(fabs(y[i]), fabs(k5[i]));
 #if !DRIFT_EXACT_ARITH
-            double inv_sk = 1.0 / sk;
+            double inv_sk = fast_rcp(sk);
 #endif
             double erri = k4[i] - BHH1 * k1[i] - BHH2 * k9[i] - BHH3 * k3[i];
 #if DRIFT_EXACT_ARITH

@@ -14,6 +14,8 @@
 // drains.
 #pragma once
 
+#include <type_traits>
+
 #include "drift_dop853.cuh"
 #include "drift_dopr54.cuh"
 #include "drift_launch_args.cuh"
@@ -49,17 +51,27 @@ __device__ __forceinline__ int64_t claim_particle(unsigned long long *cursor)
 #define DRIFT_MIN_BLOCKS_PER_SM 3
 #endif
 
-// Dynamic shared memory per block: the DOP853 rcont parking tile,
-// 24 doubles per thread, column-major by thread.
-__host__ __device__ constexpr size_t park_bytes(int block) { return 24 * sizeof(double) * block; }
+// Dynamic shared memory per block: the DOP853 rcont parking tile (24
+// doubles per thread, column-major by thread), then the Bovy bulge table.
+__host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
+{
+    return (method == DRIFT_DOP853 ? 24 * sizeof(double) * block : 0) +
+           (kind == DRIFT_POT_BOVY ? sizeof(BulgeTable) : 0);
+}
 
 template <int METHOD, class Pot>
 __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
-    integrate_kernel(KernelArgs a)
+    integrate_kernel(const __grid_constant__ KernelArgs a)
 {
-    extern __shared__ double rcont_park[];
-    volatile double *park = rcont_park + threadIdx.x;
-    const Pot pot(a.potential);
+    extern __shared__ double smem[];
+    // [park tile (DOP853)][bulge table (Bovy)]
+    volatile double *park = smem + threadIdx.x;
+    double *table = smem + (METHOD == DRIFT_DOP853 ? 24 * blockDim.x : 0);
+    if (std::is_same<Pot, Bovy>::value) {
+        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
+        __syncthreads();
+    }
+    const Pot pot(a.potential, table);
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t deadline = a.timeout_ns ? global_timer_ns() + a.timeout_ns : 0;
 
@@ -183,9 +195,14 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
 
 template <class Pot>
 __global__ void __launch_bounds__(256) force_kernel(drift_potential p, int64_t n, const double *xyz,
-                                                    double *acc)
+                                                    double *acc, const __grid_constant__ BulgeTable bt)
 {
-    const Pot pot(p);
+    __shared__ double table[BULGE_TABLE_SIZE];
+    if (std::is_same<Pot, Bovy>::value) {
+        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+        __syncthreads();
+    }
+    const Pot pot(p, table);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         double ax, ay, az;
@@ -197,14 +214,14 @@ __global__ void __launch_bounds__(256) force_kernel(drift_potential p, int64_t n
 }
 
 inline cudaError_t force_impl(const drift_potential &p, int64_t n, const double *xyz, double *acc,
-                              int grid, cudaStream_t stream)
+                              const BulgeTable &bt, int grid, cudaStream_t stream)
 {
     switch (p.kind) {
-    case DRIFT_POT_KEPLER: force_kernel<KeplerGalpy><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
-    case DRIFT_POT_PLUMMER: force_kernel<Plummer><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
-    case DRIFT_POT_BOVY: force_kernel<Bovy><<<grid, 256, 0, stream>>>(p, n, xyz, acc); break;
+    case DRIFT_POT_KEPLER: force_kernel<KeplerGalpy><<<grid, 256, 0, stream>>>(p, n, xyz, acc, bt); break;
+    case DRIFT_POT_PLUMMER: force_kernel<Plummer><<<grid, 256, 0, stream>>>(p, n, xyz, acc, bt); break;
+    case DRIFT_POT_BOVY: force_kernel<Bovy><<<grid, 256, 0, stream>>>(p, n, xyz, acc, bt); break;
     case DRIFT_POT_KEPLER_CARTESIAN:
-        force_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(p, n, xyz, acc);
+        force_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(p, n, xyz, acc, bt);
         break;
     default: return cudaErrorInvalidValue;
     }
@@ -218,7 +235,7 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
     const int kind = a.potential.kind;
 #define DRIFT_LAUNCH(M, P)                                                       \
     do {                                                                         \
-        integrate_kernel<M, P><<<grid, block, M == DRIFT_DOP853 ? park_bytes(block) : 0, stream>>>(a); \
+        integrate_kernel<M, P><<<grid, block, smem_bytes(M, kind, block), stream>>>(a); \
         return cudaGetLastError();                                               \
     } while (0)
 #define DRIFT_POT_SWITCH(M)                                                      \
@@ -244,7 +261,7 @@ inline cudaError_t occupancy_impl(int method, int kind, int block, int *blocks_p
 {
 #define DRIFT_OCC(M, P)                                                                     \
     return cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                   \
-        blocks_per_sm, integrate_kernel<M, P>, block, M == DRIFT_DOP853 ? park_bytes(block) : 0)
+        blocks_per_sm, integrate_kernel<M, P>, block, smem_bytes(M, kind, block))
 #define DRIFT_OCC_SWITCH(M)                                                     \
     switch (kind) {                                                             \
     case DRIFT_POT_KEPLER: DRIFT_OCC(M, KeplerGalpy);                           \

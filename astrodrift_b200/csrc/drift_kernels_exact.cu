@@ -11,9 +11,9 @@ cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
     return exact::launch_impl(a, method, grid, block, stream);
 }
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
-                        int grid, cudaStream_t stream)
+                        const BulgeTable &bt, int grid, cudaStream_t stream)
 {
-    return exact::force_impl(p, n, xyz, acc, grid, stream);
+    return exact::force_impl(p, n, xyz, acc, bt, grid, stream);
 }
 int max_threads_exact() { return exact::max_threads_impl(); }
 cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)

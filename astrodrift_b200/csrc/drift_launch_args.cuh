@@ -6,6 +6,7 @@
 
 #include "drift_b200.h"
 #include "drift_dopr54.cuh"
+#include "drift_potentials.cuh"
 
 namespace drift {
 
@@ -31,7 +32,11 @@ struct KernelArgs {
     uint32_t *n_rejected;
     unsigned long long *cursor;  // persistent schedule queue position (workspace)
     drift_potential potential;
+    BulgeTable bulge;            // Bovy only: lower incomplete gamma table
 };
+
+// Fill the bulge table for exponent s (host, extended precision).
+void fill_bulge_table(double s, BulgeTable *t);
 
 // Per-precision launchers (one translation unit each).
 cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
@@ -42,7 +47,7 @@ cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)
 int max_threads_exact();
 int max_threads_fma();
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
-                        int grid, cudaStream_t stream);
+                        const BulgeTable &bt, int grid, cudaStream_t stream);
 cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm);
 
 }  // namespace drift

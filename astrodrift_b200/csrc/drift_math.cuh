@@ -46,7 +46,20 @@ __device__ __forceinline__ void pow_1p5_dd(double x, double &hi, double &lo)
 
 __device__ __forceinline__ bool in_fast_range(double x)
 {
-    return x > 1e-200 && x < 1e200;
+    return __builtin_expect(x > 1e-200 && x < 1e200, 1);
+}
+
+// 1/x for x in [1e-300, 1e300] without the division's special-case branch:
+// hardware estimate (PTX rcp.approx.ftz.f64) and two Newton steps
+// r <- r (2 - x r), within about an ulp of the rounded quotient.  Used only
+// where the reference's rounding need not be reproduced.
+__device__ __forceinline__ double fast_rcp(double x)
+{
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    r = r * fma(-x, r, 2.0);
+    r = r * fma(-x, r, 2.0);
+    return r;
 }
 
 // x^(3/2), rounded to nearest (pow(x, 1.5) semantics for x >= 0).
@@ -94,7 +107,7 @@ __device__ __forceinline__ double pow_m1p5_core(double x)
 // special values: +-0 -> +inf, +inf -> +0, x < 0 -> NaN).
 __device__ __forceinline__ double pow_m1p5(double x)
 {
-    if (x > 1e-90 && x < 1e90) return pow_m1p5_core(x);
+    if (__builtin_expect(x > 1e-90 && x < 1e90, 1)) return pow_m1p5_core(x);
     if (x == 0.0) return __longlong_as_double(0x7ff0000000000000LL);  // +inf
     if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);
     if (isinf(x)) return 0.0;
@@ -108,7 +121,7 @@ __device__ __forceinline__ double pow_m1p5(double x)
 __device__ __forceinline__ double root8(double x)
 {
     double y0 = sqrt(sqrt(sqrt(x)));
-    if (!(x > 1e-280 && x < 1e300)) return y0;
+    if (__builtin_expect(!(x > 1e-280 && x < 1e300), 0)) return y0;
     double a_h, a_l, b_h, b_l, c_h, c_l;
     two_prod(y0, y0, a_h, a_l);                 // y0^2
     two_prod(a_h, a_h, b_h, b_l);               // y0^4

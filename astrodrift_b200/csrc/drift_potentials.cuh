@@ -9,13 +9,19 @@
 //   Plummer         shared/src/potential.rs:254-261
 //   Bovy            shared/src/potential.rs:117-124 = ((bulge + disk) + halo),
 //                   disk :138-151, halo :165-175, bulge = power law with
-//                   exponential cutoff (enclosed-mass force).
+//                   exponential cutoff (enclosed-mass force).  In FMA mode
+//                   (DRIFT_EXACT_ARITH 0) the disk and halo use reciprocals
+//                   and rsqrt instead of the reference's divisions.
 // pow(., -1.5) and pow(., 1.5) go through the correctly rounded routines of
 // drift_math.cuh instead of a general pow.
 #pragma once
 
 #include "drift_math.cuh"
 #include "drift_b200.h"
+
+#ifndef DRIFT_EXACT_ARITH
+#define DRIFT_EXACT_ARITH 1
+#endif
 
 // DRIFT_FORCE_NOINLINE: keep one out-of-line copy of each force body instead
 // of inlining it at every stage (the integrators evaluate it up to 17 times
@@ -30,7 +36,7 @@ namespace drift {
 
 struct KeplerGalpy {
     double amp;
-    __host__ __device__ explicit KeplerGalpy(const drift_potential &p) : amp(p.amp) {}
+    __host__ __device__ KeplerGalpy(const drift_potential &p, const double * = nullptr) : amp(p.amp) {}
     __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
@@ -51,7 +57,7 @@ struct KeplerGalpy {
 
 struct KeplerCartesian {
     double amp;
-    __host__ __device__ explicit KeplerCartesian(const drift_potential &p) : amp(p.amp) {}
+    __host__ __device__ KeplerCartesian(const drift_potential &p, const double * = nullptr) : amp(p.amp) {}
     __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
@@ -67,7 +73,10 @@ struct KeplerCartesian {
 
 struct Plummer {
     double amp, b2;
-    __host__ __device__ explicit Plummer(const drift_potential &p) : amp(p.amp), b2(p.b * p.b) {}
+    __host__ __device__ Plummer(const drift_potential &p, const double * = nullptr)
+        : amp(p.amp), b2(p.b * p.b)
+    {
+    }
     __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
@@ -79,55 +88,62 @@ struct Plummer {
     }
 };
 
-// Lower incomplete gamma gamma(s, x): power series for x < s + 1, modified
-// Lentz continued fraction for Gamma(s, x) otherwise (Numerical Recipes 3rd
-// ed. section 6.2).  Same recurrences and stopping rules as the host oracle.
-__device__ __forceinline__ double lower_gamma(double s, double x, double gamma_s)
+// Lower incomplete gamma gamma(s, x) of the bulge at fixed cost.
+//
+// The host oracle follows Numerical Recipes (series / continued fraction);
+// those loops run a data-dependent number of divisions, which diverges across
+// the lanes of a warp.  The device evaluates the same function from a table
+// built on the host in extended precision:
+//   x <  6:  gamma = x^s e^-x P(x),  P(x) = sum_n x^n / (s (s+1) ... (s+n)),
+//            a positive power series truncated at degree 40 (the omitted tail
+//            is below 1e-20 of P at x = 6);
+//   6 <= x < 40: Taylor expansion of gamma(s, .) around the centres 7, 9, ..., 39,
+//            degree 18 in t = x - centre, |t| <= 1.  gamma' = x^(s-1) e^-x is
+//            singular at 0, so the expansion converges like (|t|/centre)^k:
+//            (1/7)^19 < 1e-16;
+//   x >= 40: gamma = Gamma(s) (Gamma(s, 40) < 1e-18 Gamma(s) for s <= 1.5).
+constexpr int BULGE_SERIES_DEG = 40;
+constexpr int BULGE_PIECES = 17;
+constexpr int BULGE_PIECE_DEG = 18;
+constexpr int BULGE_TABLE_SIZE = (BULGE_SERIES_DEG + 1) + BULGE_PIECES * (BULGE_PIECE_DEG + 1);
+constexpr double BULGE_X_SERIES = 6.0;
+constexpr double BULGE_X_CONST = 40.0;
+constexpr double BULGE_FIRST_CENTRE = 7.0;
+
+struct BulgeTable {
+    double c[BULGE_TABLE_SIZE];
+};
+
+__device__ __forceinline__ double bulge_lower_gamma(const double *table, double s, double x,
+                                                    double gamma_s)
 {
-    const double eps = 1.1102230246251565e-16;  // 2^-53
-    const double fpmin = 1e-300;
-    if (!(x > 0.0)) return 0.0;
-    double prefactor = exp(s * log(x) - x);
-    if (x < s + 1.0) {
-        double ap = s;
-        double del = 1.0 / s;
-        double sum = del;
-        for (int n = 0; n < 500; ++n) {
-            ap += 1.0;
-            del *= x / ap;
-            sum += del;
-            if (fabs(del) < fabs(sum) * eps) break;
-        }
-        return sum * prefactor;
+    if (x < BULGE_X_SERIES) {
+        double p = table[BULGE_SERIES_DEG];
+#pragma unroll
+        for (int n = BULGE_SERIES_DEG - 1; n >= 0; --n) p = fma(p, x, table[n]);
+        return exp(s * log(x) - x) * p;
     }
-    if (prefactor == 0.0) return gamma_s;  // Gamma(s, x) underflows: gamma == Gamma(s)
-    double b = x + 1.0 - s;
-    double c = 1.0 / fpmin;
-    double d = 1.0 / b;
-    double h = d;
-    for (int i = 1; i < 500; ++i) {
-        double an = -i * (i - s);
-        b += 2.0;
-        d = an * d + b;
-        if (fabs(d) < fpmin) d = fpmin;
-        c = b + an / c;
-        if (fabs(c) < fpmin) c = fpmin;
-        d = 1.0 / d;
-        double del = d * c;
-        h *= del;
-        if (fabs(del - 1.0) < eps) break;
+    if (x < BULGE_X_CONST) {
+        int j = min((int)((x - (BULGE_FIRST_CENTRE - 1.0)) * 0.5), BULGE_PIECES - 1);
+        double t = x - (BULGE_FIRST_CENTRE + 2.0 * j);
+        const double *c = table + (BULGE_SERIES_DEG + 1) + j * (BULGE_PIECE_DEG + 1);
+        double p = c[BULGE_PIECE_DEG];
+#pragma unroll
+        for (int k = BULGE_PIECE_DEG - 1; k >= 0; --k) p = fma(p, t, c[k]);
+        return p;
     }
-    return gamma_s - prefactor * h;
+    return gamma_s;
 }
 
 struct Bovy {
     double mn_amp, mn_a, mn_b2;
     double nfw_amp, nfw_a;
     double bulge_s, bulge_rc2, bulge_k, bulge_gamma_s;
-    __host__ __device__ explicit Bovy(const drift_potential &p)
+    const double *table;  // BulgeTable staged in shared memory
+    __device__ Bovy(const drift_potential &p, const double *bulge_table)
         : mn_amp(p.mn_amp), mn_a(p.mn_a), mn_b2(p.mn_b * p.mn_b), nfw_amp(p.nfw_amp),
           nfw_a(p.nfw_a), bulge_s(1.5 - 0.5 * p.bulge_alpha), bulge_rc2(p.bulge_rc * p.bulge_rc),
-          bulge_k(p.bulge_k), bulge_gamma_s(p.bulge_gamma_s)
+          bulge_k(p.bulge_k), bulge_gamma_s(p.bulge_gamma_s), table(bulge_table)
     {
     }
 
@@ -139,7 +155,7 @@ struct Bovy {
         double r2s = x * x + y * y + z * z;
         if (r2s != 0.0) {
             double r = sqrt(r2s);
-            double g = lower_gamma(bulge_s, r2s / bulge_rc2, bulge_gamma_s);
+            double g = bulge_lower_gamma(table, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
             double ar_over_r = -bulge_k * g / (r2s * r);
             bx = ar_over_r * x;
             by = ar_over_r * y;
@@ -149,8 +165,9 @@ struct Bovy {
         double dx, dy, dz;
         {
             double r2 = x * x + y * y;
-            double r = sqrt(r2);
             double z2 = z * z;
+#if DRIFT_EXACT_ARITH
+            double r = sqrt(r2);
             double sqrtz2b2 = sqrt(z2 + mn_b2);
             double apz = mn_a + sqrtz2b2;
             double pyth = apz * apz;
@@ -159,16 +176,37 @@ struct Bovy {
             dx = ar * (x / r);
             dy = ar * (y / r);
             dz = -mn_amp * (z * apz) / (sqrtz2b2 * denom);
+#else
+            // a_R x/R == -amp x / D with D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
+            double inv_sz = rsqrt(z2 + mn_b2);
+            double apz = fma(z2 + mn_b2, inv_sz, mn_a);
+            double m_over_d = -mn_amp * fast_rcp(pow_1p5(fma(apz, apz, r2)));
+            dx = m_over_d * x;
+            dy = m_over_d * y;
+            dz = m_over_d * z * apz * inv_sz;
+#endif
         }
         // NFW halo
         double hx, hy, hz;
         {
             double r2 = r2s;
+#if DRIFT_EXACT_ARITH
             double r = sqrt(r2);
             double ar = -nfw_amp * (log(1. + r / nfw_a) - r / (nfw_a + r)) / r2;
             hx = ar * (x / r);
             hy = ar * (y / r);
             hz = ar * (z / r);
+#else
+            double inv_r = rsqrt(r2);
+            double r = r2 * inv_r;
+            double inv_a = fast_rcp(nfw_a);
+            double u = r * inv_a;
+            double term = log(1. + u) - u * fast_rcp(1.0 + u);
+            double ar_over_r = -nfw_amp * term * (inv_r * inv_r * inv_r);
+            hx = ar_over_r * x;
+            hy = ar_over_r * y;
+            hz = ar_over_r * z;
+#endif
         }
         ax = (bx + dx) + hx;
         ay = (by + dy) + hy;
