@@ -19,7 +19,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdrift_b200.so"
 DOPR54, DOP853 = 0, 1
 POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN = 0, 1, 2, 3
 EXACT, FMA = 0, 1
-PLAIN, PERSISTENT = 0, 1
+PLAIN, PERSISTENT, ORDERED = 0, 1, 2
 INITIAL_STEP_SENTINEL = -9999.99
 PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT = range(5)
 

@@ -139,8 +139,11 @@ int validate(const drift_launch *L, bool device_pointers)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown method");
     if (L->precision != DRIFT_PRECISION_EXACT && L->precision != DRIFT_PRECISION_FMA)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown precision");
-    if (L->schedule != DRIFT_SCHEDULE_PLAIN && L->schedule != DRIFT_SCHEDULE_PERSISTENT)
+    if (L->schedule != DRIFT_SCHEDULE_PLAIN && L->schedule != DRIFT_SCHEDULE_PERSISTENT &&
+        L->schedule != DRIFT_SCHEDULE_ORDERED)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown schedule");
+    if (L->schedule == DRIFT_SCHEDULE_ORDERED && L->n > (int64_t)UINT32_MAX)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the ordered schedule supports at most 2^32 - 1 particles");
     const int max_block = std::min(drift::max_threads_exact(), drift::max_threads_fma());
     if (L->block_size != 0 && (L->block_size < 32 || L->block_size > max_block || L->block_size % 32))
         return fail(DRIFT_ERROR_INVALID_ARGUMENT,
@@ -177,7 +180,7 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.n = L->n;
     a.y0 = L->y0;
     a.nt = (int32_t)L->nt;
-    a.persistent = L->schedule == DRIFT_SCHEDULE_PERSISTENT;
+    a.persistent = L->schedule != DRIFT_SCHEDULE_PLAIN;
     a.ts = L->ts;
     a.t0 = L->t0;
     a.t_end = L->t_end;
@@ -210,16 +213,28 @@ cudaError_t launch_args(const drift::KernelArgs &a, int method, int precision, i
                                               : drift::launch_fma(a, method, grid, block, s);
 }
 
-int grid_of(DeviceContext *ctx, const drift_launch *L, int64_t n, int block, int *grid)
+// Workspace of a request: [cursor, 256 B][ordered: bucket counts 1 KiB]
+// [ordered: queue, 4 B per particle][ordered: cost keys, 1 B per particle].
+size_t workspace_bytes(const drift_launch *L)
+{
+    if (L->schedule == DRIFT_SCHEDULE_PERSISTENT) return CURSOR_BYTES;
+    if (L->schedule == DRIFT_SCHEDULE_ORDERED) {
+        size_t b = CURSOR_BYTES + 1024 + 5 * (size_t)L->n;
+        return (b + 255) / 256 * 256;
+    }
+    return 0;
+}
+
+int grid_for(int sm_count, const drift_launch *L, int64_t n, int block, int *grid)
 {
     int64_t blocks = (n + block - 1) / block;
-    if (L->schedule == DRIFT_SCHEDULE_PERSISTENT) {
+    if (L->schedule != DRIFT_SCHEDULE_PLAIN) {
         int per_sm = 0;
         cudaError_t e = L->precision == DRIFT_PRECISION_EXACT
                             ? drift::occupancy_exact(L->method, L->potential.kind, block, &per_sm)
                             : drift::occupancy_fma(L->method, L->potential.kind, block, &per_sm);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        int64_t cap = (int64_t)std::max(per_sm, 1) * ctx->sm_count;
+        int64_t cap = (int64_t)std::max(per_sm, 1) * sm_count;
         blocks = std::min(blocks, cap);
     }
     if (blocks > INT32_MAX) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "too many particles for one launch");
@@ -227,20 +242,35 @@ int grid_of(DeviceContext *ctx, const drift_launch *L, int64_t n, int block, int
     return DRIFT_SUCCESS;
 }
 
-// Launch on device buffers.  `cursor` is needed by the persistent schedule.
-int launch_device(DeviceContext *ctx, const drift_launch *L, void *cursor, cudaStream_t s)
+// Launch on device buffers with `ws` (workspace_bytes(L) bytes, 256-byte
+// aligned) as scratch.  Every launch clears the parts that must start at 0.
+int launch_on_workspace(int sm_count, const drift_launch *L, void *ws, cudaStream_t s)
 {
     drift::KernelArgs a = make_args(L);
     const int block = block_of(L);
     int grid = 0;
-    int rc = grid_of(ctx, L, L->n, block, &grid);
+    int rc = grid_for(sm_count, L, L->n, block, &grid);
     if (rc) return rc;
     if (a.persistent) {
-        a.cursor = static_cast<unsigned long long *>(cursor);
-        DRIFT_CUDA_TRY(cudaMemsetAsync(cursor, 0, sizeof(unsigned long long), s), "cudaMemsetAsync");
+        char *base = static_cast<char *>(ws);
+        a.cursor = reinterpret_cast<unsigned long long *>(base);
+        DRIFT_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(unsigned long long), s), "cudaMemsetAsync");
+        if (L->schedule == DRIFT_SCHEDULE_ORDERED) {
+            unsigned *counts = reinterpret_cast<unsigned *>(base + CURSOR_BYTES);
+            uint32_t *order = reinterpret_cast<uint32_t *>(base + CURSOR_BYTES + 1024);
+            uint8_t *keys = reinterpret_cast<uint8_t *>(order + L->n);
+            DRIFT_CUDA_TRY(drift::build_order(a, L->method, keys, counts, order, sm_count, s),
+                           "ordering kernels");
+            a.order = order;
+        }
     }
     DRIFT_CUDA_TRY(launch_args(a, L->method, L->precision, grid, block, s), "kernel launch");
     return DRIFT_SUCCESS;
+}
+
+int launch_device(DeviceContext *ctx, const drift_launch *L, void *ws, cudaStream_t s)
+{
+    return launch_on_workspace(ctx->sm_count, L, ws, s);
 }
 
 bool is_pinned(const void *p)
@@ -332,7 +362,7 @@ int drift_potential_bovy(drift_potential *p, double alpha, double rc, double bul
 int drift_query_workspace(const drift_launch *launch, size_t *bytes)
 {
     if (!launch || !bytes) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument");
-    *bytes = launch->schedule == DRIFT_SCHEDULE_PERSISTENT ? CURSOR_BYTES : 0;
+    *bytes = workspace_bytes(launch);
     return DRIFT_SUCCESS;
 }
 
@@ -343,10 +373,12 @@ int drift_integrate(const drift_launch *launch, void *stream)
     DeviceContext *ctx = nullptr;
     rc = current_context(&ctx);
     if (rc) return rc;
-    if (launch->schedule == DRIFT_SCHEDULE_PERSISTENT) {
-        if (!launch->workspace || launch->workspace_bytes < sizeof(unsigned long long) ||
+    const size_t need = workspace_bytes(launch);
+    if (need) {
+        if (!launch->workspace || launch->workspace_bytes < need ||
             reinterpret_cast<uintptr_t>(launch->workspace) % 8)
-            return fail(DRIFT_ERROR_WORKSPACE, "persistent schedule needs an 8-byte aligned workspace of at least 8 bytes");
+            return fail(DRIFT_ERROR_WORKSPACE, "this schedule needs an 8-byte aligned workspace of " +
+                                                   std::to_string(need) + " bytes (drift_query_workspace)");
     }
     return launch_device(ctx, launch, launch->workspace, static_cast<cudaStream_t>(stream));
 }
@@ -410,27 +442,10 @@ extern "C" int drift_integrate_noalloc(const drift_launch *launch, void *stream)
     int sm_count = 0;
     DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device),
                    "cudaDeviceGetAttribute");
-
-    drift::KernelArgs a = make_args(launch);
-    const int block = block_of(launch);
-    int64_t blocks = (launch->n + block - 1) / block;
-    if (a.persistent) {
-        int per_sm = 0;
-        e = launch->precision == DRIFT_PRECISION_EXACT
-                ? drift::occupancy_exact(launch->method, launch->potential.kind, block, &per_sm)
-                : drift::occupancy_fma(launch->method, launch->potential.kind, block, &per_sm);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
-        blocks = std::min(blocks, (int64_t)std::max(per_sm, 1) * sm_count);
-    }
-    if (blocks > INT32_MAX) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "too many particles for one launch");
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
-    if (a.persistent) {
-        // The array keeps the previous call's contents; the cursor must start at 0.
-        a.cursor = static_cast<unsigned long long *>(scratch);
-        DRIFT_CUDA_TRY(cudaMemsetAsync(scratch, 0, sizeof(unsigned long long), s), "cudaMemsetAsync");
-    }
-    DRIFT_CUDA_TRY(launch_args(a, launch->method, launch->precision, (int)blocks, block, s),
-                   "kernel launch");
+    // The array keeps the previous call's contents; launch_on_workspace clears
+    // what must start at zero on the caller's stream.
+    rc = launch_on_workspace(sm_count, launch, scratch, static_cast<cudaStream_t>(stream));
+    if (rc) return rc;
     return DRIFT_SUCCESS;
 }
 
@@ -495,7 +510,7 @@ int drift_integrate_host(const drift_launch *L)
     if (L->err_code) DRIFT_CUDA_TRY(ctx->err.ensure(n * sizeof(int32_t)), "cudaMalloc(err)");
     if (L->n_accepted) DRIFT_CUDA_TRY(ctx->acc.ensure(n * sizeof(uint32_t)), "cudaMalloc(acc)");
     if (L->n_rejected) DRIFT_CUDA_TRY(ctx->rej.ensure(n * sizeof(uint32_t)), "cudaMalloc(rej)");
-    DRIFT_CUDA_TRY(ctx->cursor.ensure(2 * CURSOR_BYTES), "cudaMalloc(cursor)");
+    // (the per-slot workspace is sized once the chunk length is known)
 
     // Trajectory chunks: particles [c0, c0 + cn) write a (nt, cn, 6) device
     // block that is copied out row by row into the caller's (nt, n, 6) array.
@@ -513,6 +528,10 @@ int drift_integrate_host(const drift_launch *L)
         for (int i = 0; i < 2; i++)
             DRIFT_CUDA_TRY(ctx->out[i].ensure(chunk * nt * row), "cudaMalloc(out chunk)");
     }
+    drift_launch chunk_req = *L;
+    chunk_req.n = chunk;
+    const size_t ws_slot = std::max<size_t>(workspace_bytes(&chunk_req), CURSOR_BYTES);
+    DRIFT_CUDA_TRY(ctx->cursor.ensure(2 * ws_slot), "cudaMalloc(workspace)");
     const bool out_pinned = L->out && is_pinned(L->out);
     if (L->out && !out_pinned)
         for (int i = 0; i < 2; i++)
@@ -560,7 +579,7 @@ int drift_integrate_host(const drift_launch *L)
         sub.err_code = L->err_code ? ctx->err.as<int32_t>() + c0 : nullptr;
         sub.n_accepted = L->n_accepted ? ctx->acc.as<uint32_t>() + c0 : nullptr;
         sub.n_rejected = L->n_rejected ? ctx->rej.as<uint32_t>() + c0 : nullptr;
-        rc = launch_device(ctx, &sub, static_cast<char *>(ctx->cursor.ptr) + slot * CURSOR_BYTES, s);
+        rc = launch_device(ctx, &sub, static_cast<char *>(ctx->cursor.ptr) + slot * ws_slot, s);
         if (rc) return rc;
         if (L->out) {
             if (out_pinned) {

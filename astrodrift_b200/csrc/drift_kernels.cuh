@@ -14,6 +14,7 @@
 // drains.
 #pragma once
 
+#include <algorithm>
 #include <type_traits>
 
 #include "drift_dop853.cuh"
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
         if (a.persistent && !active && !exhausted) {
             int64_t p = claim_particle(a.cursor);
             if (p < a.n)
-                start(p);
+                start(a.order ? (int64_t)__ldg(a.order + p) : p);
             else
                 exhausted = true;
         }
@@ -191,6 +192,104 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
         else
             nrej++;
     }
+}
+
+// ---- longest-first queue (ordered schedule) ------------------------------
+//
+// Cost estimate of a particle: number of dynamical times in its time span,
+// |t_end - t0| * sqrt(|F| / r + (v / r)^2), plus nt / 4 for the output
+// intervals DOPR54 must land on.  Keys are 4 buckets per octave of cost;
+// bucket 0 holds the most expensive particles.
+constexpr int ORDER_BUCKETS = 256;
+
+template <class Pot>
+__global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ KernelArgs a, int method,
+                                                   uint8_t *keys, unsigned *counts)
+{
+    __shared__ unsigned hist[ORDER_BUCKETS];
+    __shared__ double table[BULGE_TABLE_SIZE];
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
+    if (std::is_same<Pot, Bovy>::value)
+        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
+    __syncthreads();
+    const Pot pot(a.potential, table);
+    for (int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pid < a.n;
+         pid += (int64_t)gridDim.x * blockDim.x) {
+        const double *y = a.y0 + pid * 6;
+        double span = a.ts ? fabs(__ldg(a.ts + a.nt - 1) - __ldg(a.ts)) : fabs(__ldg(a.t_end + pid) - a.t0);
+        double ax, ay, az;
+        pot.force(y[0], y[1], y[2], ax, ay, az);
+        double r2 = fmax(y[0] * y[0] + y[1] * y[1] + y[2] * y[2], 1e-300);
+        double v2 = y[3] * y[3] + y[4] * y[4] + y[5] * y[5];
+        double f = sqrt(ax * ax + ay * ay + az * az);
+        double cost = span * sqrt(f * rsqrt(r2) + v2 / r2);
+        if (method == DRIFT_DOPR54) cost += 0.25 * a.nt;
+        int key = 0;
+        if (cost > 0.0 && cost < 1e300) key = min(max((int)floor(4.0 * log2(cost)) + 128, 0), ORDER_BUCKETS - 1);
+        else if (!(cost > 0.0)) key = 0;
+        else key = ORDER_BUCKETS - 1;
+        keys[pid] = (uint8_t)key;
+        atomicAdd(&hist[ORDER_BUCKETS - 1 - key], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x)
+        if (hist[i]) atomicAdd(&counts[i], hist[i]);
+}
+
+// Exclusive prefix sum of the 256 bucket counts, in place (one block of 256).
+__global__ void __launch_bounds__(256) order_scan_kernel(unsigned *counts)
+{
+    __shared__ unsigned v[ORDER_BUCKETS];
+    const int i = threadIdx.x;
+    v[i] = counts[i];
+    __syncthreads();
+    for (int off = 1; off < ORDER_BUCKETS; off <<= 1) {
+        unsigned add = i >= off ? v[i - off] : 0u;
+        __syncthreads();
+        v[i] += add;
+        __syncthreads();
+    }
+    counts[i] = i ? v[i - 1] : 0u;
+}
+
+// order[offset[bucket]++] = pid, one atomic per (warp, bucket) group.
+__global__ void __launch_bounds__(256) order_scatter_kernel(int64_t n, const uint8_t *keys,
+                                                            unsigned *offsets, uint32_t *order)
+{
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = base + threadIdx.x;
+        const bool valid = pid < n;
+        const int bucket = valid ? ORDER_BUCKETS - 1 - keys[pid] : -1 - (int)(threadIdx.x & 31);
+        const unsigned peers = __match_any_sync(0xffffffffu, bucket);
+        if (valid) {
+            const int lane = threadIdx.x & 31;
+            const int leader = __ffs(peers) - 1;
+            unsigned pos = 0;
+            if (lane == leader) pos = atomicAdd(&offsets[bucket], (unsigned)__popc(peers));
+            pos = __shfl_sync(peers, pos, leader);
+            order[pos + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)pid;
+        }
+    }
+}
+
+inline cudaError_t build_order_impl(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                                    uint32_t *order, int sm_count, cudaStream_t stream)
+{
+    cudaError_t e = cudaMemsetAsync(counts, 0, ORDER_BUCKETS * sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const int grid = (int)std::min<int64_t>((a.n + 255) / 256, (int64_t)sm_count * 8);
+    switch (a.potential.kind) {
+    case DRIFT_POT_KEPLER: rank_kernel<KeplerGalpy><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_PLUMMER: rank_kernel<Plummer><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_BOVY: rank_kernel<Bovy><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_KEPLER_CARTESIAN:
+        rank_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(a, method, keys, counts);
+        break;
+    default: return cudaErrorInvalidValue;
+    }
+    order_scan_kernel<<<1, ORDER_BUCKETS, 0, stream>>>(counts);
+    order_scatter_kernel<<<grid, 256, 0, stream>>>(a.n, keys, counts, order);
+    return cudaGetLastError();
 }
 
 template <class Pot>

@@ -16,6 +16,11 @@ cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, 
     return exact::force_impl(p, n, xyz, acc, bt, grid, stream);
 }
 int max_threads_exact() { return exact::max_threads_impl(); }
+cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                        uint32_t *order, int sm_count, cudaStream_t stream)
+{
+    return exact::build_order_impl(a, method, keys, counts, order, sm_count, stream);
+}
 cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)
 {
     return exact::occupancy_impl(method, kind, block, blocks_per_sm);

@@ -31,6 +31,7 @@ struct KernelArgs {
     uint32_t *n_accepted;
     uint32_t *n_rejected;
     unsigned long long *cursor;  // persistent schedule queue position (workspace)
+    const uint32_t *order;       // ordered schedule: queue position -> particle, or NULL
     drift_potential potential;
     BulgeTable bulge;            // Bovy only: lower incomplete gamma table
 };
@@ -46,6 +47,11 @@ cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
 cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm);
 int max_threads_exact();
 int max_threads_fma();
+// Longest-first queue for the ordered schedule: fills order[0..n) with the
+// particles in decreasing estimated cost.  `counts` holds 256 uint32 and
+// `keys` n bytes of scratch.
+cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                        uint32_t *order, int sm_count, cudaStream_t stream);
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
                         const BulgeTable &bt, int grid, cudaStream_t stream);
 cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm);

@@ -170,7 +170,9 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         std::memset(&L, 0, sizeof(L));
         L.method = config.method == Method::DOPR54 ? DRIFT_DOPR54 : DRIFT_DOP853;
         L.precision = config.precision == Precision::EXACT ? DRIFT_PRECISION_EXACT : DRIFT_PRECISION_FMA;
-        L.schedule = config.schedule == Schedule::PLAIN ? DRIFT_SCHEDULE_PLAIN : DRIFT_SCHEDULE_PERSISTENT;
+        L.schedule = config.schedule == Schedule::PLAIN        ? DRIFT_SCHEDULE_PLAIN
+                     : config.schedule == Schedule::PERSISTENT ? DRIFT_SCHEDULE_PERSISTENT
+                                                               : DRIFT_SCHEDULE_ORDERED;
         L.block_size = config.block_size;
         L.potential = potential_of(*force_source);
         L.n = n;
@@ -203,7 +205,10 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         DRIFT_LOG(LOG_GPU, LOG_DEBUG,
                   fmt("launching %s kernel: %lld particles, block=%d, schedule=%s, %lld output times",
                       kernel_label, (long long)n, config.block_size ? config.block_size : 128,
-                      config.schedule == Schedule::PLAIN ? "plain" : "persistent", (long long)ts.steps));
+                      config.schedule == Schedule::PLAIN        ? "plain"
+                      : config.schedule == Schedule::PERSISTENT ? "persistent"
+                                                                : "ordered",
+                      (long long)ts.steps));
         if (!backend_announced) {
             DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, "context initialized and kernel module loaded (sm_100a)");
             backend_announced = true;

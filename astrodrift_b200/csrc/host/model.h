@@ -22,7 +22,7 @@ enum class Engine { CPU, GPU };
 enum class Method { DOPR54, DOP853 };
 enum class Implementation { GALPY, SCIPY, DRIFT };
 enum class Precision { EXACT, FMA };
-enum class Schedule { PLAIN, PERSISTENT };
+enum class Schedule { PLAIN, PERSISTENT, ORDERED };
 
 const char *name_of(Engine e);
 const char *name_of(Method m);
@@ -62,7 +62,7 @@ struct Config {
     OutputGrid output;
     Tolerance tolerance;
     Precision precision = Precision::EXACT;
-    Schedule schedule = Schedule::PERSISTENT;
+    Schedule schedule = Schedule::ORDERED;
     int block_size = 0;
     int64_t max_steps = 0;
     double timeout_s = 0.0;

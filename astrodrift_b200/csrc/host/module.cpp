@@ -541,8 +541,10 @@ PYBIND11_MODULE(_drift, m)
                          c.inner.schedule = Schedule::PLAIN;
                      else if (v == "persistent")
                          c.inner.schedule = Schedule::PERSISTENT;
+                     else if (v == "ordered")
+                         c.inner.schedule = Schedule::ORDERED;
                      else
-                         throw py::value_error("schedule must be 'plain' or 'persistent'");
+                         throw py::value_error("schedule must be 'plain', 'persistent' or 'ordered'");
                  }
                  if (block_size != 0 && (block_size < 32 || block_size > 128 || block_size % 32))
                      throw py::value_error("block_size must be a multiple of 32 in [32, 128]");

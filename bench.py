@@ -206,7 +206,7 @@ def main() -> None:
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--precision", default="fma", choices=["exact", "fma"])
-    ap.add_argument("--schedule", default="persistent", choices=["plain", "persistent"])
+    ap.add_argument("--schedule", default="ordered", choices=["plain", "persistent", "ordered"])
     ap.add_argument("--block", type=int, default=0)
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-sample", type=int, default=262144)
@@ -241,7 +241,7 @@ def main() -> None:
     ts = np.linspace(*TS[:2], TS[2])
     n, nt = len(y0), len(ts)
     precision = capi.EXACT if args.precision == "exact" else capi.FMA
-    schedule = capi.PLAIN if args.schedule == "plain" else capi.PERSISTENT
+    schedule = {"plain": capi.PLAIN, "persistent": capi.PERSISTENT, "ordered": capi.ORDERED}[args.schedule]
 
     y0_d = torch.from_numpy(y0).to(dev)
     ts_d = torch.from_numpy(ts).to(dev)

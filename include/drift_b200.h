@@ -67,7 +67,11 @@ typedef enum {
     DRIFT_SCHEDULE_PLAIN = 0,
     /* Persistent grid; a thread that finishes its particle takes the next one
      * from a device-wide cursor (needs workspace). */
-    DRIFT_SCHEDULE_PERSISTENT = 1
+    DRIFT_SCHEDULE_PERSISTENT = 1,
+    /* Persistent grid fed longest-first: each particle's cost is estimated
+     * from its time span and dynamical frequency at t0, and particles are
+     * claimed in decreasing cost (workspace grows by 5 bytes per particle). */
+    DRIFT_SCHEDULE_ORDERED = 2
 } drift_schedule;
 
 /* Return codes of every entry point. */
@@ -133,7 +137,7 @@ typedef struct {
     int32_t *err_code;     /* (n) galpy DOPR54 error code, or NULL */
     uint32_t *n_accepted;  /* (n) accepted steps, or NULL */
     uint32_t *n_rejected;  /* (n) rejected steps, or NULL */
-    void *workspace;       /* device scratch for the persistent schedule */
+    void *workspace;       /* device scratch for the persistent and ordered schedules */
     size_t workspace_bytes;
 } drift_launch;
 
@@ -189,15 +193,18 @@ int drift_force(const drift_potential *potential, int64_t n, const double *xyz, 
  * an allocation's implicit synchronisation would stall the pipeline, or a
  * plugin running inside another runtime that forbids allocation.  For them
  * this entry point takes the same request as drift_integrate, with device
- * pointers for every input and output, and allocates nothing: the only
- * scratch the kernels need (the persistent schedule's claim cursor) lives in
- * a fixed DRIFT_NOALLOC_SCRATCH_BYTES array inside the library, which every
+ * pointers for every input and output, and allocates nothing: the scratch
+ * the kernels need (the persistent schedule's claim cursor; for the ordered
+ * schedule also its longest-first queue, 5 bytes per particle) lives in a
+ * fixed DRIFT_NOALLOC_SCRATCH_BYTES array inside the library, which every
  * GPU that loads the library holds until the process exits.
  * launch->workspace is ignored.
  *
  * Limits and rules:
  *  - a request whose drift_query_workspace size exceeds
- *    DRIFT_NOALLOC_SCRATCH_BYTES is rejected with DRIFT_ERROR_WORKSPACE;
+ *    DRIFT_NOALLOC_SCRATCH_BYTES is rejected with DRIFT_ERROR_WORKSPACE
+ *    (plain and persistent requests always fit; ordered requests fit up to
+ *    563 particles);
  *  - the first call on a device looks up the array's device address for
  *    that device (with that device current); make that first call before
  *    any CUDA stream capture;

@@ -160,10 +160,37 @@ def test_schedules_and_block_sizes_are_bitwise_identical(cuda_device):
     y0 = np.concatenate([g["plummer_y0"]] * 5)[:301]  # ragged count
     runs = [capi.integrate_host(capi.DOP853, capi.plummer(), y0, ts=g["ts"], rtol=1e-10, atol=1e-10,
                                 schedule=s, block_size=b)
-            for s, b in ((capi.PLAIN, 0), (capi.PERSISTENT, 0), (capi.PERSISTENT, 64), (capi.PLAIN, 32))]
+            for s, b in ((capi.PLAIN, 0), (capi.PERSISTENT, 0), (capi.PERSISTENT, 64), (capi.PLAIN, 32),
+                         (capi.ORDERED, 0), (capi.ORDERED, 96))]
     for r in runs[1:]:
         np.testing.assert_array_equal(r["out"], runs[0]["out"])
         np.testing.assert_array_equal(r["accepted"], runs[0]["accepted"])
+
+
+@pytest.mark.parametrize("method", ["dopr54", "dop853"])
+def test_ordered_schedule_on_uneven_bovy_workload(oracle, cuda_device, method):
+    # Per-particle end times spanning two decades and radii spanning two:
+    # step counts differ by orders of magnitude, the case the longest-first
+    # queue is for.  Results must not depend on the schedule.
+    from astrodrift_b200.workloads import bovy_disc
+
+    m, om = METHODS[method]
+    bov = oracle.bovy()
+    fr = np.vectorize(lambda R: oracle.force(bov, R, 0.0, 0.0)[0])
+    y0, t_end = bovy_disc(3000, seed=5, radial_force=fr)
+    # U[0.2, 20]: at rtol = 1e-10 two correct integrations of these orbits stay
+    # within 1e-9 of each other over ~20 time units; over much longer spans
+    # their difference grows at the scale of the integration error, and the
+    # full-size tests check conserved quantities instead.
+    t_end = t_end / 50.0
+    runs = {s: capi.integrate_host(m, capi.bovy(), y0, t_end=t_end, nt=11, rtol=1e-10, atol=1e-10,
+                                   schedule=s)
+            for s in (capi.ORDERED, capi.PLAIN)}
+    np.testing.assert_array_equal(runs[capi.ORDERED]["out"], runs[capi.PLAIN]["out"])
+    assert (runs[capi.ORDERED]["status"] == 0).all()
+    idx = np.random.default_rng(2).choice(3000, 300, replace=False)
+    ref = oracle.integrate_batch(om, bov, y0[idx], t_end=t_end[idx], nt=11, rtol=1e-10, atol=1e-10)
+    assert rel_err(runs[capi.ORDERED]["out"][:, idx], ref["out"]) < REL_TOL
 
 
 def test_device_entry_point_matches_host_entry_point(cuda_device):

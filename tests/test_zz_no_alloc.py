@@ -82,6 +82,29 @@ def test_noalloc_matches_drift_integrate_dop853_plummer(cuda_device, schedule):
     _case(torch, capi.DOP853, capi.plummer(1.0, 1.0), y0, np.linspace(0.0, 30.0, 31), schedule)
 
 
+def test_noalloc_ordered_schedule_within_and_beyond_its_scratch(cuda_device):
+    import ctypes
+
+    import torch
+
+    rng = np.random.default_rng(23)
+    n = 500  # the ordered queue of 500 particles fits the fixed scratch
+    r = rng.uniform(0.3, 2.0, n)
+    y0 = np.hstack([rng.normal(size=(n, 3)), rng.normal(size=(n, 3))])
+    y0[:, :3] *= (r / np.linalg.norm(y0[:, :3], axis=1))[:, None]
+    y0[:, 3:] *= 0.3 / np.linalg.norm(y0[:, 3:], axis=1)[:, None]
+    _case(torch, capi.DOP853, capi.plummer(1.0, 1.0), y0, np.linspace(0.0, 10.0, 11), capi.ORDERED)
+
+    # A queue too large for the fixed scratch is refused with a clear error.
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 100_000, 11, rtol=1e-10, atol=1e-10,
+                         schedule=capi.ORDERED)
+    dummy = torch.zeros(16, dtype=torch.float64, device="cuda:0")
+    L.y0, L.ts, L.out = dummy.data_ptr(), dummy.data_ptr(), dummy.data_ptr()
+    rc = capi.lib().drift_integrate_noalloc(ctypes.byref(L), None)
+    assert rc == 3  # DRIFT_ERROR_WORKSPACE
+    assert "fixed scratch" in capi.lib().drift_last_error().decode()
+
+
 def test_noalloc_matches_drift_integrate_dopr54_kepler(cuda_device):
     import torch
 
