@@ -40,6 +40,7 @@ CUDA_UNITS = {
     "drift_kernels_exact": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "drift_kernels_fma": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "drift_capi": [],
+    "drift_server": [],
 }
 
 

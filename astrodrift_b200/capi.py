@@ -38,6 +38,12 @@ EXPORTED = (
     "drift_galpy_dop853",
     "drift_force",
     "drift_integrate_noalloc",
+    "drift_integrate_batch",
+    "drift_server_create",
+    "drift_server_submit",
+    "drift_server_wait",
+    "drift_server_stats_get",
+    "drift_server_destroy",
 )
 
 
@@ -113,6 +119,7 @@ def lib() -> ctypes.CDLL:
         L.drift_force.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int64, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p]
         L.drift_integrate_noalloc.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
+        L.drift_integrate_batch.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_int32, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -225,6 +232,13 @@ def integrate_device_noalloc(L: DriftLaunch, stream: int = 0) -> None:
     """drift_integrate_noalloc on device pointers already stored in ``L`` (no workspace)."""
     check(lib().drift_integrate_noalloc(ctypes.byref(L), ctypes.c_void_p(stream)),
           "drift_integrate_noalloc")
+
+
+def integrate_batch_device(launches: list, stream: int = 0) -> None:
+    """drift_integrate_batch on device pointers already stored in each launch."""
+    arr = (DriftLaunch * len(launches))(*launches)
+    check(lib().drift_integrate_batch(arr, len(launches), ctypes.c_void_p(stream)),
+          "drift_integrate_batch")
 
 
 def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream: int = 0) -> None:

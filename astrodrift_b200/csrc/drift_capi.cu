@@ -242,11 +242,12 @@ int grid_for(int sm_count, const drift_launch *L, int64_t n, int block, int *gri
     return DRIFT_SUCCESS;
 }
 
-// Launch on device buffers with `ws` (workspace_bytes(L) bytes, 256-byte
+// Launch prepared kernel arguments `a` for request geometry `L` (n = all
+// particles of the launch) with `ws` (workspace_bytes(L) bytes, 256-byte
 // aligned) as scratch.  Every launch clears the parts that must start at 0.
-int launch_on_workspace(int sm_count, const drift_launch *L, void *ws, cudaStream_t s)
+int launch_args_on_workspace(int sm_count, const drift_launch *L, drift::KernelArgs &a, void *ws,
+                             cudaStream_t s)
 {
-    drift::KernelArgs a = make_args(L);
     const int block = block_of(L);
     int grid = 0;
     int rc = grid_for(sm_count, L, L->n, block, &grid);
@@ -268,6 +269,65 @@ int launch_on_workspace(int sm_count, const drift_launch *L, void *ws, cudaStrea
     return DRIFT_SUCCESS;
 }
 
+int launch_on_workspace(int sm_count, const drift_launch *L, void *ws, cudaStream_t s)
+{
+    drift::KernelArgs a = make_args(L);
+    return launch_args_on_workspace(sm_count, L, a, ws, s);
+}
+
+// A batch of requests sharing method, precision, schedule, block size,
+// potential, tolerances and step limits, as one launch over their
+// concatenated particles.  Request i occupies [first_i, first_i + n_i).
+int check_batch(const drift_launch *R, int32_t count)
+{
+    if (!R || count < 1 || count > drift::MAX_BATCH)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "a batch holds 1 to " + std::to_string(drift::MAX_BATCH) + " requests");
+    for (int32_t i = 0; i < count; i++) {
+        int rc = validate(&R[i], true);
+        if (rc) return rc;
+        const drift_launch &A = R[0], &B = R[i];
+        if (B.method != A.method || B.precision != A.precision || B.schedule != A.schedule ||
+            B.block_size != A.block_size || std::memcmp(&B.potential, &A.potential, sizeof(A.potential)) ||
+            B.rtol_ln != A.rtol_ln || B.atol_ln != A.atol_ln || B.dt_one != A.dt_one ||
+            B.max_steps != A.max_steps || B.timeout_s != A.timeout_s)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                        "batched requests must share method, precision, schedule, block size, "
+                        "potential, tolerances, first step and limits");
+    }
+    if (R[0].schedule == DRIFT_SCHEDULE_ORDERED)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "batched launches use the plain or persistent schedule");
+    return DRIFT_SUCCESS;
+}
+
+int launch_batch(int sm_count, const drift_launch *R, int32_t count, void *ws, cudaStream_t s)
+{
+    drift::KernelArgs a = make_args(&R[0]);
+    drift_launch geometry = R[0];
+    int64_t first = 0;
+    a.nsegs = count;
+    for (int32_t i = 0; i < count; i++) {
+        drift::Segment &S = a.segs[i];
+        S.first = first;
+        S.n = R[i].n;
+        S.y0 = R[i].y0;
+        S.ts = R[i].ts;
+        S.t0 = R[i].t0;
+        S.t_end = R[i].t_end;
+        S.nt = (int32_t)R[i].nt;
+        S.out = R[i].out;
+        S.y_final = R[i].y_final;
+        S.status = R[i].status;
+        S.err_code = R[i].err_code;
+        S.n_accepted = R[i].n_accepted;
+        S.n_rejected = R[i].n_rejected;
+        first += R[i].n;
+    }
+    a.n = first;
+    geometry.n = first;
+    return launch_args_on_workspace(sm_count, &geometry, a, ws, s);
+}
+
 int launch_device(DeviceContext *ctx, const drift_launch *L, void *ws, cudaStream_t s)
 {
     return launch_on_workspace(ctx->sm_count, L, ws, s);
@@ -285,6 +345,17 @@ bool is_pinned(const void *p)
 
 }  // namespace
 
+// Shared with the request server (drift_server.cu).
+int drift_internal_launch_batch(int sm_count, const drift_launch *R, int32_t count, void *ws,
+                                cudaStream_t s)
+{
+    int rc = check_batch(R, count);
+    if (rc) return rc;
+    return launch_batch(sm_count, R, count, ws, s);
+}
+
+int drift_internal_fail(int code, const char *msg) { return fail(code, msg); }
+
 extern "C" {
 
 int drift_abi_version(void) { return DRIFT_ABI_VERSION; }
@@ -298,6 +369,8 @@ const char *drift_result_string(int code)
     case DRIFT_ERROR_WORKSPACE: return "workspace too small";
     case DRIFT_ERROR_NO_DEVICE: return "no CUDA device";
     case DRIFT_ERROR_OUT_OF_MEMORY: return "out of device memory";
+    case DRIFT_ERROR_TIMEOUT: return "timed out";
+    case DRIFT_ERROR_CANCELLED: return "cancelled";
     default: return "unknown error";
     }
 }
@@ -450,6 +523,22 @@ extern "C" int drift_integrate_noalloc(const drift_launch *launch, void *stream)
 }
 
 extern "C" {
+
+int drift_integrate_batch(const drift_launch *requests, int32_t count, void *stream)
+{
+    int rc = check_batch(requests, count);
+    if (rc) return rc;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    if (requests[0].schedule == DRIFT_SCHEDULE_PERSISTENT &&
+        (!requests[0].workspace || requests[0].workspace_bytes < CURSOR_BYTES ||
+         reinterpret_cast<uintptr_t>(requests[0].workspace) % 8))
+        return fail(DRIFT_ERROR_WORKSPACE, "a persistent batch needs requests[0].workspace of " +
+                                               std::to_string(CURSOR_BYTES) + " bytes");
+    return launch_batch(ctx->sm_count, requests, count, requests[0].workspace,
+                        static_cast<cudaStream_t>(stream));
+}
 
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream)

@@ -94,12 +94,40 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
     uint32_t nacc = 0, nrej = 0;
     bool active = false;
 
+    int32_t seg = 0;  // batched launches: request of the current particle
+
     auto start = [&](int64_t p) {
+        const double *y0p;
+        if (a.nsegs) {
+            // Last request whose first index is <= p.
+            int lo = 0, hi = a.nsegs - 1;
+            while (lo < hi) {
+                int mid = (lo + hi + 1) >> 1;
+                if (a.segs[mid].first <= p)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            seg = lo;
+            const Segment &S = a.segs[seg];
+            p -= S.first;
+            grid.ts = S.ts;
+            grid.t0 = S.t0;
+            grid.nt = S.nt;
+            grid.t_end = S.ts ? 0.0 : S.t_end[p];
+            out.base = S.out;
+            out.y_final = S.y_final;
+            out.n = S.n;
+            out.nt = S.nt;
+            y0p = S.y0 + p * 6;
+        } else {
+            if (!a.ts) grid.t_end = __ldg(a.t_end + p);
+            y0p = a.y0 + p * 6;
+        }
         pid = p;
         out.pid = p;
-        if (!a.ts) grid.t_end = __ldg(a.t_end + p);
         double y0[6];
-        const double2 *src = reinterpret_cast<const double2 *>(a.y0 + p * 6);
+        const double2 *src = reinterpret_cast<const double2 *>(y0p);
 #pragma unroll
         for (int i = 0; i < 3; i++) {
             double2 v = __ldg(src + i);
@@ -123,17 +151,27 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
 #pragma unroll
             for (int i = 0; i < 6; i++) nan6[i] = __longlong_as_double(0x7ff8000000000000LL);
             int32_t first = (METHOD == DRIFT_DOP853) ? l853.next + 1 : l54.ii + 1;
-            for (int32_t k = first; k < a.nt; k++) out.write(k, nan6);
+            for (int32_t k = first; k < grid.nt; k++) out.write(k, nan6);
         }
         int32_t code = 0;
         if (METHOD == DRIFT_DOPR54) {
             code = l54.err;
             if (status == DRIFT_PARTICLE_OK && (code & 1)) status = DRIFT_PARTICLE_MIN_STEP;
         }
-        if (a.status) a.status[pid] = (uint8_t)status;
-        if (a.err_code) a.err_code[pid] = code;
-        if (a.n_accepted) a.n_accepted[pid] = nacc;
-        if (a.n_rejected) a.n_rejected[pid] = nrej;
+        uint8_t *st = a.status;
+        int32_t *ec = a.err_code;
+        uint32_t *na = a.n_accepted, *nr = a.n_rejected;
+        if (a.nsegs) {
+            const Segment &S = a.segs[seg];
+            st = S.status;
+            ec = S.err_code;
+            na = S.n_accepted;
+            nr = S.n_rejected;
+        }
+        if (st) st[pid] = (uint8_t)status;
+        if (ec) ec[pid] = code;
+        if (na) na[pid] = nacc;
+        if (nr) nr[pid] = nrej;
         active = false;
     };
 

@@ -10,6 +10,29 @@
 
 namespace drift {
 
+// Requests one batched launch can carry; the table travels in the kernel's
+// parameter space (MAX_BATCH x 104 bytes), so no device table is needed.
+constexpr int MAX_BATCH = DRIFT_MAX_BATCH;  // from drift_b200.h
+
+// One request of a batched launch: particles [first, first + n) of the
+// launch's index space, with the request's own inputs, grid and outputs.
+struct Segment {
+    int64_t first;
+    int64_t n;
+    const double *y0;         // (n, 6)
+    const double *ts;         // shared grid of this request, or NULL
+    double t0;                // per-particle grid start (ts == NULL)
+    const double *t_end;      // (n) per-particle grid ends (ts == NULL)
+    int32_t nt;
+    int32_t reserved;
+    double *out;              // (nt, n, 6) or NULL
+    double *y_final;          // (n, 6) or NULL
+    uint8_t *status;
+    int32_t *err_code;
+    uint32_t *n_accepted;
+    uint32_t *n_rejected;
+};
+
 // Everything a launch needs, passed by value as the kernel parameter.
 struct KernelArgs {
     int64_t n;
@@ -32,8 +55,10 @@ struct KernelArgs {
     uint32_t *n_rejected;
     unsigned long long *cursor;  // persistent schedule queue position (workspace)
     const uint32_t *order;       // ordered schedule: queue position -> particle, or NULL
+    int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
     drift_potential potential;
     BulgeTable bulge;            // Bovy only: lower incomplete gamma table
+    Segment segs[MAX_BATCH];  // batched launch: the request table (kernel parameter space)
 };
 
 // Fill the bulge table for exponent s (host, extended precision).

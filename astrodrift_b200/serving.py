@@ -1,0 +1,150 @@
+"""Python handle on the request server of the C ABI (drift_server_*).
+
+    with Server(memory_bytes=8 << 30, streams=4) as srv:
+        req = srv.submit(capi.DOP853, capi.plummer(), y0, ts=ts, rtol=1e-10, atol=1e-10)
+        res = req.wait()            # dict of numpy arrays + "latency_s"
+
+Requests keep their host buffers alive until they complete; trajectory
+buffers are page-locked (allocated by the library) so the server's copies
+overlap the integration of other requests.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import capi
+
+
+class ServerOptions(ctypes.Structure):
+    _fields_ = [
+        ("memory_fraction", ctypes.c_double),
+        ("memory_bytes", ctypes.c_size_t),
+        ("streams", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("max_batch_particles", ctypes.c_int64),
+    ]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_uint64) for name in (
+        "requests_submitted", "requests_completed", "requests_pending", "particles_completed",
+        "batches_launched", "pieces_launched", "batches_in_flight", "bytes_to_device",
+        "bytes_to_host", "memory_budget", "bytes_in_flight", "peak_bytes_in_flight")]
+
+
+def _lib():
+    L = capi.lib()
+    if not getattr(L, "_server_bound", False):
+        L.drift_server_create.argtypes = [ctypes.POINTER(ServerOptions), ctypes.POINTER(ctypes.c_void_p)]
+        L.drift_server_submit.argtypes = [ctypes.c_void_p, ctypes.POINTER(capi.DriftLaunch),
+                                          ctypes.POINTER(ctypes.c_uint64)]
+        L.drift_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
+                                        ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+        L.drift_server_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+        L.drift_server_destroy.argtypes = [ctypes.c_void_p]
+        L._server_bound = True
+    return L
+
+
+class PinnedArray:
+    """A numpy view of page-locked host memory from drift_host_alloc."""
+
+    def __init__(self, shape, dtype=np.float64):
+        self.nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self.ptr = ctypes.c_void_p()
+        capi.check(capi.lib().drift_host_alloc(max(self.nbytes, 1), ctypes.byref(self.ptr)),
+                   "drift_host_alloc")
+        buf = (ctypes.c_char * max(self.nbytes, 1)).from_address(self.ptr.value)
+        buf._owner = self  # the numpy view keeps this object, hence the memory, alive
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    def free(self):
+        if self.ptr:
+            capi.lib().drift_host_free(self.ptr)
+            self.ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Request:
+    def __init__(self, server, ticket, keep, arrays):
+        self.server, self.ticket, self._keep, self.arrays = server, ticket, keep, arrays
+
+    def wait(self, timeout: float = 0.0) -> dict:
+        if not self.server._ptr:
+            raise RuntimeError("the server is closed")
+        result = ctypes.c_int(0)
+        latency = ctypes.c_double(0.0)
+        capi.check(_lib().drift_server_wait(self.server._ptr, self.ticket, timeout, ctypes.byref(result),
+                                            ctypes.byref(latency)), "drift_server_wait")
+        if result.value != 0:
+            raise RuntimeError(f"request failed: {capi.lib().drift_result_string(result.value).decode()}")
+        out = dict(self.arrays)
+        out["latency_s"] = latency.value
+        self._keep = None
+        return out
+
+
+class Server:
+    def __init__(self, memory_fraction: float = 0.5, memory_bytes: int = 0, streams: int = 4,
+                 max_batch_particles: int = 1 << 20):
+        opts = ServerOptions(memory_fraction=memory_fraction, memory_bytes=memory_bytes,
+                             streams=streams, max_batch_particles=max_batch_particles)
+        self._ptr = ctypes.c_void_p()
+        capi.check(_lib().drift_server_create(ctypes.byref(opts), ctypes.byref(self._ptr)),
+                   "drift_server_create")
+
+    def submit(self, method, pot, y0, *, ts=None, t_end=None, nt=None, t0=0.0, rtol=1e-12,
+               atol=1e-12, precision=capi.EXACT, out=None, want_out=True) -> Request:
+        y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
+        n = y0.shape[0]
+        if ts is not None:
+            ts = np.ascontiguousarray(ts, dtype=np.float64)
+            nt = len(ts)
+        else:
+            t_end = np.ascontiguousarray(t_end, dtype=np.float64)
+        L = capi.make_launch(method, pot, n, nt, rtol=rtol, atol=atol, precision=precision,
+                             schedule=capi.PERSISTENT, t0=t0)
+        arrays = dict(
+            y_final=np.empty((n, 6)), status=np.empty(n, np.uint8), err=np.empty(n, np.int32),
+            accepted=np.empty(n, np.uint32), rejected=np.empty(n, np.uint32))
+        pinned = None
+        if want_out:
+            if out is None:
+                pinned = PinnedArray((nt, n, 6))
+                out = pinned.array
+                pinned = None  # lifetime follows the returned array
+            arrays["out"] = out
+        L.y0, L.ts, L.t_end = y0.ctypes.data, (ts.ctypes.data if ts is not None else None), (
+            t_end.ctypes.data if t_end is not None else None)
+        L.out = out.ctypes.data if want_out else None
+        L.y_final = arrays["y_final"].ctypes.data
+        L.status, L.err_code = arrays["status"].ctypes.data, arrays["err"].ctypes.data
+        L.n_accepted, L.n_rejected = arrays["accepted"].ctypes.data, arrays["rejected"].ctypes.data
+        ticket = ctypes.c_uint64(0)
+        capi.check(_lib().drift_server_submit(self._ptr, ctypes.byref(L), ctypes.byref(ticket)),
+                   "drift_server_submit")
+        return Request(self, ticket.value, (y0, ts, t_end, L, pinned), arrays)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        capi.check(_lib().drift_server_stats_get(self._ptr, ctypes.byref(st)), "drift_server_stats_get")
+        return {name: getattr(st, name) for name, _ in ServerStats._fields_}
+
+    def close(self):
+        if self._ptr:
+            _lib().drift_server_destroy(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

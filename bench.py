@@ -199,6 +199,138 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_serving(args) -> None:
+    """Serving workload: a Poisson request stream through the request server.
+
+    Each request: N = floor(2^U[0,20]) particles; potential uniform in
+    {Kepler(1), Plummer(1,1), Bovy}; method uniform in {DOPR54, DOP853};
+    nt = floor(exp(U[ln 2, ln 10001])) outputs on (0, t_end), t_end ~ U[10, 100];
+    rtol = atol uniform in {1e-8, 1e-10, 1e-12}; exact arithmetic.  The
+    trajectory of one request is capped at 2^30 bytes (nt reduced), so every
+    result can be returned to host memory.  Latency is submission to
+    completion (results in host memory).  The same requests are then run one
+    after another through drift_integrate_host with the plain schedule: the
+    serial plain-launch baseline.
+    """
+    import ctypes
+
+    import torch
+
+    from astrodrift_b200 import capi
+    from astrodrift_b200.serving import PinnedArray, Server
+    from astrodrift_b200.workloads import bovy_disc, kepler_disc, plummer_sphere
+
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(args.seed)
+    cap_bytes = 1 << 30
+    pools = [capi.kepler(1.0), capi.plummer(1.0, 1.0), capi.bovy()]
+    bovy_fr = None
+    reqs = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / args.rate)
+        if t > args.duration:
+            break
+        n = int(2 ** rng.uniform(0, 20))
+        kind = int(rng.integers(3))
+        method = int(rng.integers(2))
+        nt = int(np.exp(rng.uniform(np.log(2), np.log(10001))))
+        nt = max(2, min(nt, cap_bytes // (48 * n)))
+        rtol = float([1e-8, 1e-10, 1e-12][int(rng.integers(3))])
+        t_end = float(rng.uniform(10.0, 100.0))
+        seed = int(rng.integers(1 << 31))
+        if kind == 0:
+            y0 = kepler_disc(n, seed=seed)
+        elif kind == 1:
+            y0 = plummer_sphere(n, seed=seed)
+        else:
+            if bovy_fr is None:
+                fr_pot = capi.bovy()
+                def bovy_fr(R):
+                    xyz = torch.zeros((len(R), 3), dtype=torch.float64, device="cuda")
+                    xyz[:, 0] = torch.from_numpy(np.asarray(R, dtype=np.float64))
+                    acc = torch.empty_like(xyz)
+                    capi.force_device(fr_pot, len(R), xyz.data_ptr(), acc.data_ptr())
+                    torch.cuda.synchronize()
+                    return acc[:, 0].cpu().numpy()
+            y0, _ = bovy_disc(n, seed=seed, radial_force=bovy_fr)
+        reqs.append(dict(at=t, method=method, pot=pools[kind], kind=kind, y0=y0,
+                         ts=np.linspace(0.0, t_end, nt), rtol=rtol))
+    # page-locked result buffers, reused across requests
+    slots = [PinnedArray((cap_bytes // 8,)) for _ in range(args.result_buffers)]
+    free_slots = list(range(len(slots)))
+
+    lat, waits, accepted_total = [], [], 0
+    with Server(memory_fraction=0.6, streams=args.streams) as srv:
+        t_begin = time.perf_counter()
+        inflight = []
+        for r in reqs:
+            while time.perf_counter() - t_begin < r["at"]:
+                time.sleep(0.0005)
+            t_want = time.perf_counter()
+            while not free_slots:
+                h, slot, rr = inflight.pop(0)
+                res = h.wait()
+                lat.append(res["latency_s"])
+                accepted_total += int(res["accepted"].astype(np.int64).sum())
+                free_slots.append(slot)
+            waits.append(time.perf_counter() - t_want)
+            slot = free_slots.pop()
+            nt, n = len(r["ts"]), len(r["y0"])
+            out = slots[slot].array[: nt * n * 6].reshape(nt, n, 6)
+            h = srv.submit(r["method"], r["pot"], r["y0"], ts=r["ts"], rtol=r["rtol"], atol=r["rtol"],
+                           out=out)
+            inflight.append((h, slot, r))
+        for h, slot, rr in inflight:
+            res = h.wait()
+            lat.append(res["latency_s"])
+            accepted_total += int(res["accepted"].astype(np.int64).sum())
+        t_served = time.perf_counter() - t_begin
+        st = srv.stats()
+    served_rate = accepted_total / t_served
+
+    # serial plain launches of the same requests
+    t0 = time.perf_counter()
+    serial_acc = 0
+    for r in reqs:
+        nt, n = len(r["ts"]), len(r["y0"])
+        res = capi.integrate_host(r["method"], r["pot"], r["y0"], ts=r["ts"], rtol=r["rtol"],
+                                  atol=r["rtol"], schedule=capi.PLAIN,
+                                  out=slots[0].array[: nt * n * 6].reshape(nt, n, 6))
+        serial_acc += int(res["accepted"].astype(np.int64).sum())
+    t_serial = time.perf_counter() - t0
+    lat_ms = np.array(lat) * 1e3
+    line = {
+        "metric": "accepted steps/s (served request stream)",
+        "value": served_rate,
+        "unit": "accepted steps/s",
+        "n_gpus": 1,
+        "steps": len(reqs),
+        "warmup": 0,
+        "ms_per_step": 1e3 * t_served / max(len(reqs), 1),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded request stream)",
+        "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
+                   "requests": len(reqs), "streams": args.streams, "precision": "exact",
+                   "trajectory_cap_bytes": cap_bytes},
+        "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                       "mean": float(lat_ms.mean()), "max": float(lat_ms.max())},
+        "client_buffer_wait_ms_p99": float(np.percentile(np.array(waits) * 1e3, 99)),
+        "serial_plain": {"value": serial_acc / t_serial, "seconds": t_serial},
+        "served_seconds": t_served,
+        "server": {k: int(v) for k, v in st.items()},
+    }
+    print(json.dumps(line), flush=True)
+    for s_ in slots:
+        s_.free()
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -215,9 +347,19 @@ def main() -> None:
     ap.add_argument("--no-peak", action="store_true", help="skip the FP64 peak probe (profiling runs)")
     ap.add_argument("--particles", type=int, default=N_PARTICLES,
                     help="particles per GPU (default: the workload's 2^20; smaller for ncu captures)")
+    ap.add_argument("--workload", default="plummer", choices=["plummer", "serving"],
+                    help="plummer: the benchmark configuration; serving: a Poisson request stream")
+    ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=20.0, help="serving: arrival window in seconds")
+    ap.add_argument("--streams", type=int, default=4, help="serving: batches in flight")
+    ap.add_argument("--result-buffers", type=int, default=16, help="serving: 1 GiB pinned result buffers")
+    ap.add_argument("--seed", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+        return
+    if args.workload == "serving":
+        run_serving(args)
         return
 
     import torch

@@ -81,7 +81,9 @@ typedef enum {
     DRIFT_ERROR_CUDA = 2,
     DRIFT_ERROR_WORKSPACE = 3,
     DRIFT_ERROR_NO_DEVICE = 4,
-    DRIFT_ERROR_OUT_OF_MEMORY = 5
+    DRIFT_ERROR_OUT_OF_MEMORY = 5,
+    DRIFT_ERROR_TIMEOUT = 6,
+    DRIFT_ERROR_CANCELLED = 7
 } drift_result;
 
 /* Per-particle status codes written to drift_launch.status. */
@@ -174,6 +176,20 @@ int drift_integrate(const drift_launch *launch, void *stream);
  * particle chunks whose copies overlap the integration of other chunks. */
 int drift_integrate_host(const drift_launch *launch);
 
+/* Largest number of requests one drift_integrate_batch launch carries. */
+#define DRIFT_MAX_BATCH 64
+
+/* Several requests as one launch over their concatenated particles, with one
+ * claim queue, so small requests share the GPU instead of each launching a
+ * mostly idle grid.  Device pointers.  The requests must share method,
+ * precision, schedule (plain or persistent), block size, potential,
+ * tolerances, first step and limits; each has its own particles, output grid
+ * and output buffers.  A persistent batch uses requests[0].workspace
+ * (drift_query_workspace of any one request).  No counterpart in the
+ * reference, which launches one kernel per stage
+ * (src/dispatch/gpu.rs:157-178). */
+int drift_integrate_batch(const drift_launch *requests, int32_t count, void *stream);
+
 /* Acceleration of the potential at n positions: xyz (n, 3) -> acc (n, 3),
  * device pointers, the same force code the integrators inline (rounded
  * without multiply-add contraction).  The reference exposes the force only
@@ -213,6 +229,51 @@ int drift_force(const drift_potential *potential, int64_t n, const double *xyz, 
  *    (different streams, or different host threads) race with each other:
  *    order them on one stream or serialise them. */
 int drift_integrate_noalloc(const drift_launch *launch, void *stream);
+
+/* ---- Request server (continuous batching) -------------------------------
+ *
+ * A resident server keeps a device memory pool, several streams and a
+ * scheduler thread.  Submitted requests (host pointers, which must stay
+ * valid until the request completes) are admitted by free device memory:
+ * whenever a stream is free, the oldest pending request and every later one
+ * that can share its launch (same method, precision, potential, tolerances
+ * and limits) form one batched launch, and requests larger than the free
+ * budget run in particle chunks.  Requests that arrive while others run start
+ * as soon as a stream and memory free up; their kernels overlap the running
+ * ones.  Trajectory buffers should be page-locked (drift_host_alloc):
+ * copies into pageable memory hold the scheduler until they finish.  Results
+ * are identical to drift_integrate_host's for the same request.  No
+ * counterpart in the reference (which runs one blocking call per stage). */
+typedef struct drift_server drift_server;
+
+typedef struct {
+    double memory_fraction;      /* of the device's free memory at creation; default 0.5 */
+    size_t memory_bytes;         /* absolute budget, overrides the fraction when > 0 */
+    int32_t streams;             /* batches in flight; default 4 */
+    int32_t reserved;
+    int64_t max_batch_particles; /* particles per launch; default 2^20 */
+} drift_server_options;
+
+typedef struct {
+    uint64_t requests_submitted, requests_completed, requests_pending;
+    uint64_t particles_completed;
+    uint64_t batches_launched, pieces_launched, batches_in_flight;
+    uint64_t bytes_to_device, bytes_to_host;
+    uint64_t memory_budget, bytes_in_flight, peak_bytes_in_flight;
+} drift_server_stats;
+
+int drift_server_create(const drift_server_options *options, drift_server **server);
+/* Plain or persistent schedule; the request's workspace is ignored. */
+int drift_server_submit(drift_server *server, const drift_launch *request, uint64_t *ticket);
+/* Blocks until the request completes (timeout_s <= 0: no limit; else
+ * DRIFT_ERROR_TIMEOUT).  request_result receives the request's drift_result,
+ * latency_s the time from submission to completion.  Releases the ticket. */
+int drift_server_wait(drift_server *server, uint64_t ticket, double timeout_s, int *request_result,
+                      double *latency_s);
+int drift_server_stats_get(drift_server *server, drift_server_stats *stats);
+/* Cancels pending requests (their waiters receive DRIFT_ERROR_CANCELLED),
+ * finishes the batches in flight and frees the server. */
+int drift_server_destroy(drift_server *server);
 
 /* The reference kernel signatures (kernels/src/lib.rs:143-173, 188-216):
  * galpy Kepler force, shared output grid, plain schedule, exact precision.
