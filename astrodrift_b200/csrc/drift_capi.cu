@@ -295,8 +295,6 @@ int check_batch(const drift_launch *R, int32_t count)
                         "batched requests must share method, precision, schedule, block size, "
                         "potential, tolerances, first step and limits");
     }
-    if (R[0].schedule == DRIFT_SCHEDULE_ORDERED)
-        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "batched launches use the plain or persistent schedule");
     return DRIFT_SUCCESS;
 }
 
@@ -531,11 +529,16 @@ int drift_integrate_batch(const drift_launch *requests, int32_t count, void *str
     DeviceContext *ctx = nullptr;
     rc = current_context(&ctx);
     if (rc) return rc;
-    if (requests[0].schedule == DRIFT_SCHEDULE_PERSISTENT &&
-        (!requests[0].workspace || requests[0].workspace_bytes < CURSOR_BYTES ||
-         reinterpret_cast<uintptr_t>(requests[0].workspace) % 8))
-        return fail(DRIFT_ERROR_WORKSPACE, "a persistent batch needs requests[0].workspace of " +
-                                               std::to_string(CURSOR_BYTES) + " bytes");
+    if (requests[0].schedule != DRIFT_SCHEDULE_PLAIN) {
+        drift_launch all = requests[0];
+        all.n = 0;
+        for (int32_t i = 0; i < count; i++) all.n += requests[i].n;
+        const size_t need = workspace_bytes(&all);
+        if (!requests[0].workspace || requests[0].workspace_bytes < need ||
+            reinterpret_cast<uintptr_t>(requests[0].workspace) % 8)
+            return fail(DRIFT_ERROR_WORKSPACE, "this batch needs an 8-byte aligned requests[0].workspace of " +
+                                                   std::to_string(need) + " bytes");
+    }
     return launch_batch(ctx->sm_count, requests, count, requests[0].workspace,
                         static_cast<cudaStream_t>(stream));
 }

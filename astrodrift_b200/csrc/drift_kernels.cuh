@@ -42,6 +42,21 @@ __device__ __forceinline__ int64_t claim_particle(unsigned long long *cursor)
     return (int64_t)(base + (unsigned long long)__popc(below));
 }
 
+// Batched launches: the request whose particles [first, first + n) hold
+// particle p (the last segment whose first index is <= p).
+__device__ __forceinline__ int segment_of(const KernelArgs &a, int64_t p)
+{
+    int lo = 0, hi = a.nsegs - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (a.segs[mid].first <= p)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 // Launch bounds of the integration kernels: at most DRIFT_MAX_THREADS
 // threads per block, and registers allocated so that DRIFT_MIN_BLOCKS_PER_SM
 // such blocks can be resident on one SM.
@@ -99,16 +114,7 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
     auto start = [&](int64_t p) {
         const double *y0p;
         if (a.nsegs) {
-            // Last request whose first index is <= p.
-            int lo = 0, hi = a.nsegs - 1;
-            while (lo < hi) {
-                int mid = (lo + hi + 1) >> 1;
-                if (a.segs[mid].first <= p)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            seg = lo;
+            seg = segment_of(a, p);
             const Segment &S = a.segs[seg];
             p -= S.first;
             grid.ts = S.ts;
@@ -253,15 +259,26 @@ __global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ Kerne
     const Pot pot(a.potential, table);
     for (int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pid < a.n;
          pid += (int64_t)gridDim.x * blockDim.x) {
-        const double *y = a.y0 + pid * 6;
-        double span = a.ts ? fabs(__ldg(a.ts + a.nt - 1) - __ldg(a.ts)) : fabs(__ldg(a.t_end + pid) - a.t0);
+        const double *y;
+        double span;
+        int64_t nt = a.nt;
+        if (a.nsegs) {
+            const Segment &S = a.segs[segment_of(a, pid)];
+            const int64_t p = pid - S.first;
+            y = S.y0 + p * 6;
+            nt = S.nt;
+            span = S.ts ? fabs(__ldg(S.ts + S.nt - 1) - __ldg(S.ts)) : fabs(__ldg(S.t_end + p) - S.t0);
+        } else {
+            y = a.y0 + pid * 6;
+            span = a.ts ? fabs(__ldg(a.ts + a.nt - 1) - __ldg(a.ts)) : fabs(__ldg(a.t_end + pid) - a.t0);
+        }
         double ax, ay, az;
         pot.force(y[0], y[1], y[2], ax, ay, az);
         double r2 = fmax(y[0] * y[0] + y[1] * y[1] + y[2] * y[2], 1e-300);
         double v2 = y[3] * y[3] + y[4] * y[4] + y[5] * y[5];
         double f = sqrt(ax * ax + ay * ay + az * az);
         double cost = span * sqrt(f * rsqrt(r2) + v2 / r2);
-        if (method == DRIFT_DOPR54) cost += 0.25 * a.nt;
+        if (method == DRIFT_DOPR54) cost += 0.25 * (double)nt;
         int key = 0;
         if (cost > 0.0 && cost < 1e300) key = min(max((int)floor(4.0 * log2(cost)) + 128, 0), ORDER_BUCKETS - 1);
         else if (!(cost > 0.0)) key = 0;

@@ -3,8 +3,8 @@
 // A scheduler thread owns a device memory pool, a set of streams and the
 // queue of submitted requests.  Whenever a stream is free it forms a batch:
 // the oldest pending request plus every later pending request that can share
-// its launch (same method, precision, potential, tolerances and limits), as
-// long as the batch fits the device-memory budget.  A request larger than the
+// its launch (same method, precision, schedule, potential, tolerances and
+// limits), as long as the batch fits the device-memory budget.  A request larger than the
 // remaining budget is admitted in particle chunks.  Each batch copies its
 // inputs in, runs one batched integration launch (drift_integrate_batch's
 // kernel path), copies trajectories and per-particle outputs back into the
@@ -83,9 +83,26 @@ size_t piece_bytes(const drift_launch &L, int64_t cn)
     return b;
 }
 
+// Schedule a request runs under inside a batch: ordered stays ordered, the
+// rest share a persistent claim queue.
+int batch_schedule(const drift_launch &L)
+{
+    return L.schedule == DRIFT_SCHEDULE_ORDERED ? DRIFT_SCHEDULE_ORDERED : DRIFT_SCHEDULE_PERSISTENT;
+}
+
+// Scratch at the front of a batch's allocation: the claim cursor, and for
+// the ordered schedule the bucket counts and the queue and keys of all its
+// particles (the layout drift_integrate_batch expects).
+size_t scratch_bytes(int schedule, int64_t particles)
+{
+    if (schedule != DRIFT_SCHEDULE_ORDERED) return CURSOR;
+    return align_up(CURSOR + 1024 + 5 * (size_t)particles);
+}
+
 bool compatible(const drift_launch &A, const drift_launch &B)
 {
     return A.method == B.method && A.precision == B.precision && A.block_size == B.block_size &&
+           batch_schedule(A) == batch_schedule(B) &&
            !std::memcmp(&A.potential, &B.potential, sizeof(A.potential)) && A.rtol_ln == B.rtol_ln &&
            A.atol_ln == B.atol_ln && A.dt_one == B.dt_one && A.max_steps == B.max_steps &&
            A.timeout_s == B.timeout_s;
@@ -167,7 +184,8 @@ struct drift_server {
         Request *head = pending.front();
         auto batch = std::make_unique<Batch>();
         size_t room = budget > bytes_inflight ? budget - bytes_inflight : 0;
-        size_t used = CURSOR;
+        const int schedule = batch_schedule(head->L);
+        size_t used = 0;  // piece bytes; the scratch goes in front of them
         int64_t particles = 0;
         std::vector<Request *> taken;
         for (Request *r : pending) {
@@ -177,10 +195,11 @@ struct drift_server {
             int64_t remaining = r->L.n - r->admitted;
             int64_t cn = std::min<int64_t>(remaining, opts.max_batch_particles - particles);
             // shrink to the memory that is left
-            while (cn > 0 && used + piece_bytes(r->L, cn) > room) cn = cn > 256 ? cn / 2 : cn - 1;
+            while (cn > 0 && scratch_bytes(schedule, particles + cn) + used + piece_bytes(r->L, cn) > room)
+                cn = cn > 256 ? cn / 2 : cn - 1;
             if (cn <= 0) {
                 if (r == head) {
-                    if (inflight.empty() && CURSOR + piece_bytes(r->L, 1) > budget) {
+                    if (inflight.empty() && scratch_bytes(schedule, 1) + piece_bytes(r->L, 1) > budget) {
                         // Not even one particle fits the whole budget.
                         r->result = DRIFT_ERROR_OUT_OF_MEMORY;
                         r->done = true;
@@ -223,6 +242,12 @@ struct drift_server {
         }
         if (batch->pieces.empty()) return false;
         for (Request *r : taken) pending.erase(std::find(pending.begin(), pending.end(), r));
+        const size_t scratch = scratch_bytes(schedule, particles);
+        for (Piece &p : batch->pieces)
+            for (size_t *o : {&p.off_y0, &p.off_grid, &p.off_out, &p.off_fin, &p.off_st, &p.off_err,
+                              &p.off_acc, &p.off_rej})
+                *o += scratch;
+        used += scratch;
 
         cudaStream_t s = streams[slot];
         void *dmem = nullptr;
@@ -230,7 +255,7 @@ struct drift_server {
             cudaGetLastError();
             // give the pieces back and wait for memory
             for (Piece &p : batch->pieces) p.req->admitted = p.c0;
-            for (Request *r : taken) pending.push_front(r);
+            for (auto it = taken.rbegin(); it != taken.rend(); ++it) pending.push_front(*it);
             return false;
         }
         batch->slot = slot;
@@ -262,9 +287,9 @@ struct drift_server {
             D.err_code = L.err_code ? reinterpret_cast<int32_t *>(base + p.off_err) : nullptr;
             D.n_accepted = L.n_accepted ? reinterpret_cast<uint32_t *>(base + p.off_acc) : nullptr;
             D.n_rejected = L.n_rejected ? reinterpret_cast<uint32_t *>(base + p.off_rej) : nullptr;
-            D.schedule = DRIFT_SCHEDULE_PERSISTENT;
+            D.schedule = schedule;
             D.workspace = base;
-            D.workspace_bytes = CURSOR;
+            D.workspace_bytes = scratch;
         }
         int rc = drift_internal_launch_batch(sm_count, sub.data(), (int32_t)sub.size(), base, s);
         for (size_t i = 0; i < batch->pieces.size(); i++) {
@@ -382,7 +407,8 @@ int drift_server_submit(drift_server *s, const drift_launch *request, uint64_t *
     if (!s || !request || !ticket)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument");
     const drift_launch &L = *request;
-    if (L.n < 1 || L.nt < 2 || !L.y0 || (!L.ts && !L.t_end) || L.schedule == DRIFT_SCHEDULE_ORDERED ||
+    if (L.n < 1 || L.nt < 2 || !L.y0 || (!L.ts && !L.t_end) || L.schedule < DRIFT_SCHEDULE_PLAIN ||
+        L.schedule > DRIFT_SCHEDULE_ORDERED ||
         L.method < DRIFT_DOPR54 || L.method > DRIFT_DOP853 || L.precision < 0 || L.precision > 1 ||
         L.potential.kind < DRIFT_POT_KEPLER || L.potential.kind > DRIFT_POT_KEPLER_CARTESIAN)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "invalid request");

@@ -102,7 +102,11 @@ class Server:
                    "drift_server_create")
 
     def submit(self, method, pot, y0, *, ts=None, t_end=None, nt=None, t0=0.0, rtol=1e-12,
-               atol=1e-12, precision=capi.EXACT, out=None, want_out=True) -> Request:
+               atol=1e-12, precision=capi.EXACT, schedule=capi.ORDERED, out=None,
+               want_out=True) -> Request:
+        """Queue one request.  ``schedule``: ORDERED batches rank their
+        particles most expensive first; PLAIN and PERSISTENT requests share a
+        persistent claim queue."""
         y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
         n = y0.shape[0]
         if ts is not None:
@@ -111,10 +115,12 @@ class Server:
         else:
             t_end = np.ascontiguousarray(t_end, dtype=np.float64)
         L = capi.make_launch(method, pot, n, nt, rtol=rtol, atol=atol, precision=precision,
-                             schedule=capi.PERSISTENT, t0=t0)
+                             schedule=schedule, t0=t0)
+        # Page-locked so the server's copies run asynchronously.
         arrays = dict(
-            y_final=np.empty((n, 6)), status=np.empty(n, np.uint8), err=np.empty(n, np.int32),
-            accepted=np.empty(n, np.uint32), rejected=np.empty(n, np.uint32))
+            y_final=PinnedArray((n, 6)).array, status=PinnedArray((n,), np.uint8).array,
+            err=PinnedArray((n,), np.int32).array, accepted=PinnedArray((n,), np.uint32).array,
+            rejected=PinnedArray((n,), np.uint32).array)
         pinned = None
         if want_out:
             if out is None:

@@ -199,41 +199,28 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
-def run_serving(args) -> None:
-    """Serving workload: a Poisson request stream through the request server.
-
-    Each request: N = floor(2^U[0,20]) particles; potential uniform in
-    {Kepler(1), Plummer(1,1), Bovy}; method uniform in {DOPR54, DOP853};
-    nt = floor(exp(U[ln 2, ln 10001])) outputs on (0, t_end), t_end ~ U[10, 100];
-    rtol = atol uniform in {1e-8, 1e-10, 1e-12}; exact arithmetic.  The
-    trajectory of one request is capped at 2^30 bytes (nt reduced), so every
-    result can be returned to host memory.  Latency is submission to
-    completion (results in host memory).  The same requests are then run one
-    after another through drift_integrate_host with the plain schedule: the
-    serial plain-launch baseline.
-    """
-    import ctypes
-
+def _serving_requests(args, capi, cap_bytes):
+    """The seeded request mix of the serving workload (arrival times in units
+    of the mean inter-arrival gap)."""
     import torch
 
-    from astrodrift_b200 import capi
-    from astrodrift_b200.serving import PinnedArray, Server
     from astrodrift_b200.workloads import bovy_disc, kepler_disc, plummer_sphere
 
-    world, rank, local = _dist()
-    if rank != 0:
-        return
-    torch.cuda.set_device(local)
     rng = np.random.default_rng(args.seed)
-    cap_bytes = 1 << 30
     pools = [capi.kepler(1.0), capi.plummer(1.0, 1.0), capi.bovy()]
-    bovy_fr = None
-    reqs = []
-    t = 0.0
-    while True:
-        t += rng.exponential(1.0 / args.rate)
-        if t > args.duration:
-            break
+    fr_pot = capi.bovy()
+
+    def bovy_fr(R):
+        xyz = torch.zeros((len(R), 3), dtype=torch.float64, device="cuda")
+        xyz[:, 0] = torch.from_numpy(np.asarray(R, dtype=np.float64))
+        acc = torch.empty_like(xyz)
+        capi.force_device(fr_pot, len(R), xyz.data_ptr(), acc.data_ptr())
+        torch.cuda.synchronize()
+        return acc[:, 0].cpu().numpy()
+
+    reqs, t = [], 0.0
+    for _ in range(args.requests):
+        t += rng.exponential(1.0)
         n = int(2 ** rng.uniform(0, 20))
         kind = int(rng.integers(3))
         method = int(rng.integers(2))
@@ -247,83 +234,151 @@ def run_serving(args) -> None:
         elif kind == 1:
             y0 = plummer_sphere(n, seed=seed)
         else:
-            if bovy_fr is None:
-                fr_pot = capi.bovy()
-                def bovy_fr(R):
-                    xyz = torch.zeros((len(R), 3), dtype=torch.float64, device="cuda")
-                    xyz[:, 0] = torch.from_numpy(np.asarray(R, dtype=np.float64))
-                    acc = torch.empty_like(xyz)
-                    capi.force_device(fr_pot, len(R), xyz.data_ptr(), acc.data_ptr())
-                    torch.cuda.synchronize()
-                    return acc[:, 0].cpu().numpy()
             y0, _ = bovy_disc(n, seed=seed, radial_force=bovy_fr)
         reqs.append(dict(at=t, method=method, pot=pools[kind], kind=kind, y0=y0,
                          ts=np.linspace(0.0, t_end, nt), rtol=rtol))
+    return reqs
+
+
+def run_serving(args) -> None:
+    """Serving workload: a request stream through the resident request server.
+
+    Each request: N = floor(2^U[0,20]) particles; potential uniform in
+    {Kepler(1), Plummer(1,1), Bovy}; method uniform in {DOPR54, DOP853};
+    nt = floor(exp(U[ln 2, ln 10001])) outputs on (0, t_end), t_end ~ U[10, 100];
+    rtol = atol uniform in {1e-8, 1e-10, 1e-12}.  One request's trajectory is
+    capped at --trajectory-cap-mib (nt reduced) so every result can be
+    returned to host memory.
+
+    Three passes over the same requests:
+      serial     -- one drift_integrate_host call per request, plain schedule,
+                    one after another (the serial plain-launch baseline; its
+                    per-request times are each request's latency alone);
+      saturated  -- every request submitted to the server at once: aggregate
+                    throughput under continuous batching;
+      open loop  -- Poisson arrivals at each offered load in --loads, as a
+                    fraction of the saturated capacity: p50/p99 latency
+                    (submission to results in host memory).
+    """
+    import torch
+
+    from astrodrift_b200 import capi
+    from astrodrift_b200.serving import PinnedArray, Server
+
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    cap_bytes = args.trajectory_cap_mib << 20
+    precision = capi.EXACT if args.precision == "exact" else capi.FMA
+    reqs = _serving_requests(args, capi, cap_bytes)
+    n_particles = sum(len(r["y0"]) for r in reqs)
+    print(f"serving: {len(reqs)} requests, {n_particles} particles", file=sys.stderr, flush=True)
     # page-locked result buffers, reused across requests
     slots = [PinnedArray((cap_bytes // 8,)) for _ in range(args.result_buffers)]
-    free_slots = list(range(len(slots)))
 
-    lat, waits, accepted_total = [], [], 0
-    with Server(memory_fraction=0.6, streams=args.streams) as srv:
-        t_begin = time.perf_counter()
-        inflight = []
-        for r in reqs:
-            while time.perf_counter() - t_begin < r["at"]:
-                time.sleep(0.0005)
-            t_want = time.perf_counter()
-            while not free_slots:
-                h, slot, rr = inflight.pop(0)
-                res = h.wait()
-                lat.append(res["latency_s"])
-                accepted_total += int(res["accepted"].astype(np.int64).sum())
-                free_slots.append(slot)
-            waits.append(time.perf_counter() - t_want)
-            slot = free_slots.pop()
-            nt, n = len(r["ts"]), len(r["y0"])
-            out = slots[slot].array[: nt * n * 6].reshape(nt, n, 6)
-            h = srv.submit(r["method"], r["pot"], r["y0"], ts=r["ts"], rtol=r["rtol"], atol=r["rtol"],
-                           out=out)
-            inflight.append((h, slot, r))
-        for h, slot, rr in inflight:
-            res = h.wait()
-            lat.append(res["latency_s"])
-            accepted_total += int(res["accepted"].astype(np.int64).sum())
-        t_served = time.perf_counter() - t_begin
-        st = srv.stats()
-    served_rate = accepted_total / t_served
-
-    # serial plain launches of the same requests
-    t0 = time.perf_counter()
-    serial_acc = 0
-    for r in reqs:
+    def out_view(slot, r):
         nt, n = len(r["ts"]), len(r["y0"])
+        return slots[slot].array[: nt * n * 6].reshape(nt, n, 6)
+
+    # warm-up: load every kernel instance once
+    for pot in (capi.kepler(1.0), capi.plummer(1.0, 1.0), capi.bovy()):
+        for method in (capi.DOPR54, capi.DOP853):
+            capi.integrate_host(method, pot, reqs[0]["y0"][:1], ts=np.linspace(0, 1, 3), rtol=1e-8,
+                                atol=1e-8, precision=precision, schedule=capi.PLAIN)
+            capi.integrate_host(method, pot, reqs[0]["y0"][:1], ts=np.linspace(0, 1, 3), rtol=1e-8,
+                                atol=1e-8, precision=precision, schedule=capi.PERSISTENT)
+
+    # serial plain launches
+    alone, serial_acc = [], 0
+    t0 = time.perf_counter()
+    for r in reqs:
+        ti = time.perf_counter()
         res = capi.integrate_host(r["method"], r["pot"], r["y0"], ts=r["ts"], rtol=r["rtol"],
-                                  atol=r["rtol"], schedule=capi.PLAIN,
-                                  out=slots[0].array[: nt * n * 6].reshape(nt, n, 6))
+                                  atol=r["rtol"], precision=precision, schedule=capi.PLAIN,
+                                  out=out_view(0, r))
+        alone.append(time.perf_counter() - ti)
         serial_acc += int(res["accepted"].astype(np.int64).sum())
     t_serial = time.perf_counter() - t0
-    lat_ms = np.array(lat) * 1e3
+    print(f"serving: serial {t_serial:.2f} s", file=sys.stderr, flush=True)
+
+    def stream(srv, gap_s):
+        """Submit every request at its arrival time (gap_s = 0: all at once);
+        returns (seconds, accepted steps, latencies, client buffer waits)."""
+        free_slots = list(range(len(slots)))
+        inflight, lat, waits, acc = [], {}, [], 0
+
+        def retire():
+            nonlocal acc
+            h, slot, i = inflight.pop(0)
+            res = h.wait()
+            lat[i] = res["latency_s"]
+            acc += int(res["accepted"].astype(np.int64).sum())
+            free_slots.append(slot)
+
+        t_begin = time.perf_counter()
+        for i, r in enumerate(reqs):
+            while time.perf_counter() - t_begin < r["at"] * gap_s:
+                time.sleep(0.0002)
+            t_want = time.perf_counter()
+            while not free_slots:
+                retire()
+            waits.append(time.perf_counter() - t_want)
+            slot = free_slots.pop()
+            h = srv.submit(r["method"], r["pot"], r["y0"], ts=r["ts"], rtol=r["rtol"], atol=r["rtol"],
+                           precision=precision, out=out_view(slot, r))
+            inflight.append((h, slot, i))
+        while inflight:
+            retire()
+        return time.perf_counter() - t_begin, acc, [lat[i] for i in range(len(reqs))], waits
+
+    with Server(memory_fraction=0.6, streams=args.streams) as srv:
+        t_sat, sat_acc, sat_lat, _ = stream(srv, 0.0)
+        print(f"serving: saturated {t_sat:.2f} s", file=sys.stderr, flush=True)
+        loads = []
+        for load in [float(x) for x in args.loads.split(",") if x]:
+            rate = load * len(reqs) / t_sat
+            t_run, acc, lat, waits = stream(srv, 1.0 / rate)
+            lat_ms = np.array(lat) * 1e3
+            slow = np.array(lat) / np.maximum(np.array(alone), 1e-9)
+            loads.append({
+                "offered_load": load, "rate_per_s": rate, "seconds": t_run,
+                "accepted_steps_per_s": acc / t_run,
+                "latency_ms": {"p50": float(np.percentile(lat_ms, 50)),
+                               "p99": float(np.percentile(lat_ms, 99)),
+                               "mean": float(lat_ms.mean()), "max": float(lat_ms.max())},
+                "slowdown_vs_alone": {"p50": float(np.percentile(slow, 50)),
+                                      "p99": float(np.percentile(slow, 99))},
+                "client_buffer_wait_ms_p99": float(np.percentile(np.array(waits) * 1e3, 99)),
+            })
+            print(f"serving: load {load} rate {rate:.2f}/s p50 {loads[-1]['latency_ms']['p50']:.1f} ms "
+                  f"p99 {loads[-1]['latency_ms']['p99']:.1f} ms", file=sys.stderr, flush=True)
+        st = srv.stats()
+    alone_ms = np.array(alone) * 1e3
+    head = loads[0] if loads else None
     line = {
         "metric": "accepted steps/s (served request stream)",
-        "value": served_rate,
+        "value": sat_acc / t_sat,
         "unit": "accepted steps/s",
         "n_gpus": 1,
         "steps": len(reqs),
-        "warmup": 0,
-        "ms_per_step": 1e3 * t_served / max(len(reqs), 1),
+        "warmup": 1,
+        "ms_per_step": 1e3 * t_sat / len(reqs),
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
         "data": "synthetic (seeded request stream)",
-        "config": {"workload": "serving", "rate_per_s": args.rate, "duration_s": args.duration,
-                   "requests": len(reqs), "streams": args.streams, "precision": "exact",
-                   "trajectory_cap_bytes": cap_bytes},
-        "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
-                       "mean": float(lat_ms.mean()), "max": float(lat_ms.max())},
-        "client_buffer_wait_ms_p99": float(np.percentile(np.array(waits) * 1e3, 99)),
-        "serial_plain": {"value": serial_acc / t_serial, "seconds": t_serial},
-        "served_seconds": t_served,
+        "config": {"workload": "serving", "requests": len(reqs), "particles": n_particles,
+                   "streams": args.streams, "precision": args.precision,
+                   "trajectory_cap_bytes": cap_bytes, "result_buffers": args.result_buffers,
+                   "seed": args.seed},
+        "serial_plain": {"value": serial_acc / t_serial, "seconds": t_serial,
+                         "latency_alone_ms": {"p50": float(np.percentile(alone_ms, 50)),
+                                              "p99": float(np.percentile(alone_ms, 99))}},
+        "saturated": {"seconds": t_sat, "speedup_vs_serial": t_serial / t_sat},
+        "latency_ms": head["latency_ms"] if head else None,
+        "open_loop": loads,
         "server": {k: int(v) for k, v in st.items()},
     }
     print(json.dumps(line), flush=True)
@@ -349,10 +404,13 @@ def main() -> None:
                     help="particles per GPU (default: the workload's 2^20; smaller for ncu captures)")
     ap.add_argument("--workload", default="plummer", choices=["plummer", "serving"],
                     help="plummer: the benchmark configuration; serving: a Poisson request stream")
-    ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
-    ap.add_argument("--duration", type=float, default=20.0, help="serving: arrival window in seconds")
+    ap.add_argument("--requests", type=int, default=32, help="serving: requests in the stream")
+    ap.add_argument("--loads", default="0.5,0.8",
+                    help="serving: offered loads (fractions of the saturated capacity) for latency")
     ap.add_argument("--streams", type=int, default=4, help="serving: batches in flight")
-    ap.add_argument("--result-buffers", type=int, default=16, help="serving: 1 GiB pinned result buffers")
+    ap.add_argument("--trajectory-cap-mib", type=int, default=256,
+                    help="serving: largest trajectory of one request")
+    ap.add_argument("--result-buffers", type=int, default=16, help="serving: pinned result buffers")
     ap.add_argument("--seed", type=int, default=4)
     args = ap.parse_args()
     if args.impl == "reference":

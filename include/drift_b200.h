@@ -182,10 +182,12 @@ int drift_integrate_host(const drift_launch *launch);
 /* Several requests as one launch over their concatenated particles, with one
  * claim queue, so small requests share the GPU instead of each launching a
  * mostly idle grid.  Device pointers.  The requests must share method,
- * precision, schedule (plain or persistent), block size, potential,
- * tolerances, first step and limits; each has its own particles, output grid
- * and output buffers.  A persistent batch uses requests[0].workspace
- * (drift_query_workspace of any one request).  No counterpart in the
+ * precision, schedule, block size, potential, tolerances, first step and
+ * limits; each has its own particles, output grid and output buffers.  A
+ * persistent or ordered batch uses requests[0].workspace, of
+ * drift_query_workspace's size for one request holding all the batch's
+ * particles; the ordered schedule ranks the particles of all requests
+ * together (most expensive first).  No counterpart in the
  * reference, which launches one kernel per stage
  * (src/dispatch/gpu.rs:157-178). */
 int drift_integrate_batch(const drift_launch *requests, int32_t count, void *stream);

@@ -2,7 +2,8 @@
 gets alone.
 
 A heterogeneous mix (both methods, three potentials, 1 to 40,000 particles,
-shared and per-particle grids, three tolerances) is submitted from several
+shared and per-particle grids, three tolerances, ordered and persistent
+batches) is submitted from several
 threads into a server whose memory budget forces large requests into
 particle chunks and whose streams run several batches at once.  Exact
 arithmetic makes each particle's integration independent of which launch,
@@ -41,6 +42,8 @@ def _mix(seed=0, count=24):
         kw = dict(method=[capi.DOPR54, capi.DOP853][i % 2], pot=pots[(i // 2) % 3], y0=y0,
                   rtol=[1e-8, 1e-10, 1e-12][i % 3])
         kw["atol"] = kw["rtol"]
+        if i % 5 == 0:
+            kw["schedule"] = capi.PERSISTENT  # the rest use the server's default, ordered
         if i % 4 == 3:
             kw.update(t_end=rng.uniform(1.0, 6.0, n), nt=max(nt, 2))
         else:
@@ -50,7 +53,7 @@ def _mix(seed=0, count=24):
 
 
 def _alone(kw):
-    args = {k: v for k, v in kw.items() if k not in ("method", "pot", "y0")}
+    args = {k: v for k, v in kw.items() if k not in ("method", "pot", "y0", "schedule")}
     return capi.integrate_host(kw["method"], kw["pot"], kw["y0"], schedule=capi.PLAIN, **args)
 
 
