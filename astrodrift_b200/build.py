@@ -39,6 +39,8 @@ CUDA_UNITS = {
     # precision-exact kernels: no contraction, IEEE division/sqrt, no flush-to-zero
     "drift_kernels_exact": ["-fmad=false", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "drift_kernels_fma": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
+    # discrete adjoint (gradients: contraction allowed)
+    "drift_adjoint": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "drift_capi": [],
     "drift_server": [],
 }

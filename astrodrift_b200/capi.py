@@ -21,7 +21,9 @@ POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN = 0, 1, 2, 3
 EXACT, FMA = 0, 1
 PLAIN, PERSISTENT, ORDERED = 0, 1, 2
 INITIAL_STEP_SENTINEL = -9999.99
-PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT = range(5)
+(PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT,
+ PARTICLE_TAPE_FULL) = range(6)
+ADJOINT_MAX_PARAMS = 6
 
 # Every symbol the header declares.
 EXPORTED = (
@@ -44,6 +46,7 @@ EXPORTED = (
     "drift_server_wait",
     "drift_server_stats_get",
     "drift_server_destroy",
+    "drift_integrate_adjoint",
 )
 
 
@@ -91,6 +94,28 @@ class DriftLaunch(ctypes.Structure):
         ("n_rejected", ctypes.c_void_p),
         ("workspace", ctypes.c_void_p),
         ("workspace_bytes", ctypes.c_size_t),
+        ("tape", ctypes.c_void_p),
+        ("tape_steps", ctypes.c_int64),
+    ]
+
+
+class DriftAdjointLaunch(ctypes.Structure):
+    _fields_ = [
+        ("method", ctypes.c_int32),
+        ("block_size", ctypes.c_int32),
+        ("potential", DriftPotential),
+        ("n", ctypes.c_int64),
+        ("nt", ctypes.c_int64),
+        ("ts", ctypes.c_void_p),
+        ("t0", ctypes.c_double),
+        ("t_end", ctypes.c_void_p),
+        ("tape", ctypes.c_void_p),
+        ("tape_steps", ctypes.c_int64),
+        ("n_accepted", ctypes.c_void_p),
+        ("status", ctypes.c_void_p),
+        ("grad_out", ctypes.c_void_p),
+        ("grad_y0", ctypes.c_void_p),
+        ("grad_params", ctypes.c_void_p),
     ]
 
 
@@ -120,6 +145,7 @@ def lib() -> ctypes.CDLL:
                                   ctypes.c_void_p, ctypes.c_void_p]
         L.drift_integrate_noalloc.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
         L.drift_integrate_batch.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_int32, ctypes.c_void_p]
+        L.drift_integrate_adjoint.argtypes = [ctypes.POINTER(DriftAdjointLaunch), ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -250,3 +276,9 @@ def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream
 def exported_symbols() -> dict[str, bool]:
     L = lib()
     return {name: hasattr(L, name) for name in EXPORTED}
+
+
+def integrate_adjoint_device(A: DriftAdjointLaunch, stream: int = 0) -> None:
+    """drift_integrate_adjoint on device pointers already stored in ``A``."""
+    check(lib().drift_integrate_adjoint(ctypes.byref(A), ctypes.c_void_p(stream)),
+          "drift_integrate_adjoint")

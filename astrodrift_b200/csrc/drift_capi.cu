@@ -164,6 +164,16 @@ int validate(const drift_launch *L, bool device_pointers)
         (reinterpret_cast<uintptr_t>(L->y0) % 16 || (L->out && reinterpret_cast<uintptr_t>(L->out) % 16) ||
          (L->y_final && reinterpret_cast<uintptr_t>(L->y_final) % 16)))
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0, out and y_final must be 16-byte aligned");
+    if (L->tape) {
+        if (!device_pointers)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the step tape is a device buffer (device entry points only)");
+        if (L->method != DRIFT_DOP853)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the step tape is recorded by DOP853 only");
+        if (L->tape_steps < 1 || L->tape_steps > (int64_t(1) << 40) / std::max<int64_t>(L->n, 1))
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "tape_steps must be >= 1 (and n * tape_steps <= 2^40)");
+        if (reinterpret_cast<uintptr_t>(L->tape) % 16)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the tape must be 16-byte aligned");
+    }
     return DRIFT_SUCCESS;
 }
 
@@ -200,6 +210,8 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.err_code = L->err_code;
     a.n_accepted = L->n_accepted;
     a.n_rejected = L->n_rejected;
+    a.tape = L->tape;
+    a.tape_steps = L->tape_steps;
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
@@ -231,8 +243,10 @@ int grid_for(int sm_count, const drift_launch *L, int64_t n, int block, int *gri
     if (L->schedule != DRIFT_SCHEDULE_PLAIN) {
         int per_sm = 0;
         cudaError_t e = L->precision == DRIFT_PRECISION_EXACT
-                            ? drift::occupancy_exact(L->method, L->potential.kind, block, &per_sm)
-                            : drift::occupancy_fma(L->method, L->potential.kind, block, &per_sm);
+                            ? drift::occupancy_exact(L->method, L->potential.kind, block, L->tape != nullptr,
+                                                     &per_sm)
+                            : drift::occupancy_fma(L->method, L->potential.kind, block, L->tape != nullptr,
+                                                   &per_sm);
         if (e != cudaSuccess) return cuda_fail(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor");
         int64_t cap = (int64_t)std::max(per_sm, 1) * sm_count;
         blocks = std::min(blocks, cap);
@@ -286,6 +300,7 @@ int check_batch(const drift_launch *R, int32_t count)
     for (int32_t i = 0; i < count; i++) {
         int rc = validate(&R[i], true);
         if (rc) return rc;
+        if (R[i].tape) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "batched launches record no step tape");
         const drift_launch &A = R[0], &B = R[i];
         if (B.method != A.method || B.precision != A.precision || B.schedule != A.schedule ||
             B.block_size != A.block_size || std::memcmp(&B.potential, &A.potential, sizeof(A.potential)) ||

@@ -252,9 +252,11 @@ struct Dop853Lane {
 
     // One step attempt (dop853.rs:425-782).  Returns true when accepted.
     // `park` is this thread's column of a [24][blockDim.x] shared tile.
-    template <class Out>
+    // TAPE: an accepted step also writes (t_old, h, y_old[6]) to tape_row.
+    template <bool TAPE = false, class Out>
     __device__ __forceinline__ bool step(const Pot &pot, const Grid &grid, double rtol,
-                                         double atol, Out &out, volatile double *park)
+                                         double atol, Out &out, volatile double *park,
+                                         double *tape_row = nullptr)
     {
         using namespace dop853c;
         const int RCONT_STRIDE = blockDim.x;
@@ -353,6 +355,13 @@ struct Dop853Lane {
 
         if (err <= 1.0) {
             nonfinite_run = 0;
+            if (TAPE) {
+                double2 *row = reinterpret_cast<double2 *>(tape_row);
+                row[0] = make_double2(t_old, h);
+                row[1] = make_double2(y[0], y[1]);
+                row[2] = make_double2(y[2], y[3]);
+                row[3] = make_double2(y[4], y[5]);
+            }
             rhs(pot, k5, k4);  // FSAL: k4 = f(t_new, y_new)
 
 #pragma unroll

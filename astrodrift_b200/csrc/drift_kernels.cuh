@@ -75,10 +75,14 @@ __host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
            (kind == DRIFT_POT_BOVY ? sizeof(BulgeTable) : 0);
 }
 
-template <int METHOD, class Pot>
+// TAPE (DOP853 only): record every accepted step of every particle in
+// a.tape for the adjoint pass; a particle whose tape is full stops with
+// DRIFT_PARTICLE_TAPE_FULL.
+template <int METHOD, class Pot, bool TAPE = false>
 __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
     integrate_kernel(const __grid_constant__ KernelArgs a)
 {
+    static_assert(!TAPE || METHOD == DRIFT_DOP853, "the step tape is recorded by DOP853 only");
     extern __shared__ double smem[];
     // [park tile (DOP853)][bulge table (Bovy)]
     volatile double *park = smem + threadIdx.x;
@@ -218,10 +222,19 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
             if (!a.persistent) exhausted = true;
             continue;
         }
+        if (TAPE && (int64_t)nacc >= a.tape_steps) {
+            finish(DRIFT_PARTICLE_TAPE_FULL);
+            if (!a.persistent) exhausted = true;
+            continue;
+        }
         attempts++;
         bool accepted;
         if (METHOD == DRIFT_DOP853) {
-            accepted = l853.step(pot, grid, a.rtol, a.atol, out, park);
+            if (TAPE)
+                accepted = l853.template step<true>(pot, grid, a.rtol, a.atol, out, park,
+                                                    a.tape + (pid * a.tape_steps + nacc) * 8);
+            else
+                accepted = l853.step(pot, grid, a.rtol, a.atol, out, park);
             if (!accepted && l853.nonfinite_run >= DOP853_NONFINITE_LIMIT) {
                 nrej++;
                 finish(DRIFT_PARTICLE_NONFINITE);
@@ -387,10 +400,14 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
                                cudaStream_t stream)
 {
     const int kind = a.potential.kind;
-#define DRIFT_LAUNCH(M, P)                                                       \
-    do {                                                                         \
-        integrate_kernel<M, P><<<grid, block, smem_bytes(M, kind, block), stream>>>(a); \
-        return cudaGetLastError();                                               \
+#define DRIFT_LAUNCH(M, P)                                                                   \
+    do {                                                                                     \
+        if (M == DRIFT_DOP853 && a.tape)                                                     \
+            integrate_kernel<DRIFT_DOP853, P, true>                                          \
+                <<<grid, block, smem_bytes(M, kind, block), stream>>>(a);                    \
+        else                                                                                 \
+            integrate_kernel<M, P><<<grid, block, smem_bytes(M, kind, block), stream>>>(a); \
+        return cudaGetLastError();                                                           \
     } while (0)
 #define DRIFT_POT_SWITCH(M)                                                      \
     switch (kind) {                                                              \
@@ -411,11 +428,15 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
 
 inline int max_threads_impl() { return DRIFT_MAX_THREADS; }
 
-inline cudaError_t occupancy_impl(int method, int kind, int block, int *blocks_per_sm)
+inline cudaError_t occupancy_impl(int method, int kind, int block, bool tape, int *blocks_per_sm)
 {
 #define DRIFT_OCC(M, P)                                                                     \
-    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(                                   \
-        blocks_per_sm, integrate_kernel<M, P>, block, smem_bytes(M, kind, block))
+    return (M == DRIFT_DOP853 && tape)                                                      \
+               ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(                             \
+                     blocks_per_sm, integrate_kernel<DRIFT_DOP853, P, true>, block,         \
+                     smem_bytes(M, kind, block))                                            \
+               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(                             \
+                     blocks_per_sm, integrate_kernel<M, P>, block, smem_bytes(M, kind, block))
 #define DRIFT_OCC_SWITCH(M)                                                     \
     switch (kind) {                                                             \
     case DRIFT_POT_KEPLER: DRIFT_OCC(M, KeplerGalpy);                           \

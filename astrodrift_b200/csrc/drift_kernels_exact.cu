@@ -21,8 +21,8 @@ cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned
 {
     return exact::build_order_impl(a, method, keys, counts, order, sm_count, stream);
 }
-cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm)
+cudaError_t occupancy_exact(int method, int kind, int block, bool tape, int *blocks_per_sm)
 {
-    return exact::occupancy_impl(method, kind, block, blocks_per_sm);
+    return exact::occupancy_impl(method, kind, block, tape, blocks_per_sm);
 }
 }  // namespace drift

@@ -10,8 +10,8 @@ cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
     return fma_mode::launch_impl(a, method, grid, block, stream);
 }
 int max_threads_fma() { return fma_mode::max_threads_impl(); }
-cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm)
+cudaError_t occupancy_fma(int method, int kind, int block, bool tape, int *blocks_per_sm)
 {
-    return fma_mode::occupancy_impl(method, kind, block, blocks_per_sm);
+    return fma_mode::occupancy_impl(method, kind, block, tape, blocks_per_sm);
 }
 }  // namespace drift

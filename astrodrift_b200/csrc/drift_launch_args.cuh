@@ -55,6 +55,8 @@ struct KernelArgs {
     uint32_t *n_rejected;
     unsigned long long *cursor;  // persistent schedule queue position (workspace)
     const uint32_t *order;       // ordered schedule: queue position -> particle, or NULL
+    double *tape;                // DOP853 step tape (t_old, h, y_old[6]) per accepted step, or NULL
+    int64_t tape_steps;          // tape rows per particle
     int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
     drift_potential potential;
     BulgeTable bulge;            // Bovy only: lower incomplete gamma table
@@ -69,7 +71,7 @@ cudaError_t launch_exact(const KernelArgs &a, int method, int grid, int block,
                          cudaStream_t stream);
 cudaError_t launch_fma(const KernelArgs &a, int method, int grid, int block,
                        cudaStream_t stream);
-cudaError_t occupancy_exact(int method, int kind, int block, int *blocks_per_sm);
+cudaError_t occupancy_exact(int method, int kind, int block, bool tape, int *blocks_per_sm);
 int max_threads_exact();
 int max_threads_fma();
 // Longest-first queue for the ordered schedule: fills order[0..n) with the
@@ -79,6 +81,6 @@ cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned
                         uint32_t *order, int sm_count, cudaStream_t stream);
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
                         const BulgeTable &bt, int grid, cudaStream_t stream);
-cudaError_t occupancy_fma(int method, int kind, int block, int *blocks_per_sm);
+cudaError_t occupancy_fma(int method, int kind, int block, bool tape, int *blocks_per_sm);
 
 }  // namespace drift

@@ -408,7 +408,7 @@ int drift_server_submit(drift_server *s, const drift_launch *request, uint64_t *
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument");
     const drift_launch &L = *request;
     if (L.n < 1 || L.nt < 2 || !L.y0 || (!L.ts && !L.t_end) || L.schedule < DRIFT_SCHEDULE_PLAIN ||
-        L.schedule > DRIFT_SCHEDULE_ORDERED ||
+        L.schedule > DRIFT_SCHEDULE_ORDERED || L.tape ||
         L.method < DRIFT_DOPR54 || L.method > DRIFT_DOP853 || L.precision < 0 || L.precision > 1 ||
         L.potential.kind < DRIFT_POT_KEPLER || L.potential.kind > DRIFT_POT_KEPLER_CARTESIAN)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "invalid request");

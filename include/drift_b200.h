@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DRIFT_ABI_VERSION 1
+#define DRIFT_ABI_VERSION 2
 
 /* Sentinel that asks DOPR54 for galpy's RK4 initial-step estimate
  * (src/integrators/galpy/mod.rs:8). */
@@ -97,7 +97,9 @@ typedef enum {
     /* DOP853's error estimate stayed non-finite for 64 consecutive attempts. */
     DRIFT_PARTICLE_NONFINITE = 3,
     /* The launch deadline passed before this particle finished. */
-    DRIFT_PARTICLE_TIMEOUT = 4
+    DRIFT_PARTICLE_TIMEOUT = 4,
+    /* The step tape (drift_launch.tape) was full before the particle finished. */
+    DRIFT_PARTICLE_TAPE_FULL = 5
 } drift_particle_status;
 
 /* Potential descriptor.  Fields a kind does not use are ignored. */
@@ -141,6 +143,12 @@ typedef struct {
     uint32_t *n_rejected;  /* (n) rejected steps, or NULL */
     void *workspace;       /* device scratch for the persistent and ordered schedules */
     size_t workspace_bytes;
+    /* DOP853 step tape for drift_integrate_adjoint, or NULL: particle i
+     * records accepted step j as 8 doubles (t_old, h, y_old[6]) at
+     * tape[(i * tape_steps + j) * 8].  Device entry points only; not with
+     * batched launches. */
+    double *tape;
+    int64_t tape_steps;
 } drift_launch;
 
 /* Library / device information. */
@@ -198,6 +206,46 @@ int drift_integrate_batch(const drift_launch *requests, int32_t count, void *str
  * through its Potential trait (shared/src/potential.rs:41-44). */
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream);
+
+/* ---- discrete adjoint (no counterpart in the reference) ----------------- */
+
+/* Largest number of potential parameters with a gradient:
+ *   Kepler (both forms): amp
+ *   Plummer:             amp, b
+ *   Bovy:                mn_amp, mn_a, mn_b, nfw_amp, nfw_a, bulge_k */
+#define DRIFT_ADJOINT_MAX_PARAMS 6
+
+/* Reverse pass of a taped DOP853 integration.  The trajectory `out` of a
+ * drift_integrate call with a tape is a function of y0 and the potential
+ * parameters through the recorded steps (the step sizes are held fixed, so
+ * this is the exact derivative of the discrete map that produced `out`).
+ * Given the cotangent grad_out of `out`, the kernel replays every particle's
+ * steps in reverse from the tape, recomputing each step's stages, and writes
+ *   grad_y0[i]     = d<grad_out, out> / d y0[i]
+ *   grad_params[i] = d<grad_out[:, i], out[:, i]> / d params   (per particle;
+ *                    the gradient of the whole trajectory is their sum).
+ * Particles whose forward status is not DRIFT_PARTICLE_OK get NaN rows.  The
+ * output grid must be monotone in the direction of integration.  Device
+ * pointers. */
+typedef struct {
+    int32_t method;            /* DRIFT_DOP853 */
+    int32_t block_size;        /* 0 = library default */
+    drift_potential potential; /* as in the forward launch */
+    int64_t n;
+    int64_t nt;
+    const double *ts;          /* grid exactly as in the forward launch */
+    double t0;
+    const double *t_end;
+    const double *tape;        /* the forward launch's tape and tape_steps */
+    int64_t tape_steps;
+    const uint32_t *n_accepted;/* (n) from the forward launch */
+    const uint8_t *status;     /* (n) from the forward launch */
+    const double *grad_out;    /* (nt, n, 6) cotangent of the trajectory */
+    double *grad_y0;           /* (n, 6) */
+    double *grad_params;       /* (n, DRIFT_ADJOINT_MAX_PARAMS), or NULL */
+} drift_adjoint_launch;
+
+int drift_integrate_adjoint(const drift_adjoint_launch *adjoint, void *stream);
 
 /* Bytes of device scratch that drift_integrate_noalloc owns (per device). */
 #define DRIFT_NOALLOC_SCRATCH_BYTES 4096

@@ -643,9 +643,9 @@ static double c_min(double a, double b) { return a < b ? a : b; }
 static double c_max(double a, double b) { return a > b ? a : b; }
 static double custom_sign(double x, double y) { return y > 0.0 ? fabs(x) : -fabs(x); }
 
-int oracle_dop853(const oracle_potential *p, const double y0_in[6], int nt, const double *t,
-                  double rtol_ln, double atol_ln, int64_t max_steps, double *result,
-                  oracle_stats *stats)
+static int dop853_run(const oracle_potential *p, const double y0_in[6], int nt, const double *t,
+                      double rtol_ln, double atol_ln, int64_t max_steps, double *result,
+                      oracle_stats *stats, double *tape, int64_t tape_steps)
 {
     const int dim = DIM;
     oracle_stats local = {0, 0, 0};
@@ -779,6 +779,12 @@ int oracle_dop853(const oracle_potential *p, const double y0_in[6], int nt, cons
         double hnew = h / fac;
 
         if (err <= 1.0) {
+            if (tape && st->accepted < tape_steps) {
+                double *row = tape + st->accepted * 8;
+                row[0] = t_old;
+                row[1] = h;
+                for (i = 0; i < dim; i++) row[2 + i] = y0[i];
+            }
             st->accepted++;
             facold = c_max(err, 1.0e-4);
             rhs(p, t_current, k5, k4, st);
@@ -859,6 +865,21 @@ int oracle_dop853(const oracle_potential *p, const double y0_in[6], int nt, cons
         h = hnew;
     }
     return ORACLE_OK;
+}
+
+int oracle_dop853(const oracle_potential *p, const double y0_in[6], int nt, const double *t,
+                  double rtol_ln, double atol_ln, int64_t max_steps, double *result,
+                  oracle_stats *stats)
+{
+    return dop853_run(p, y0_in, nt, t, rtol_ln, atol_ln, max_steps, result, stats, NULL, 0);
+}
+
+int oracle_dop853_tape(const oracle_potential *p, const double y0_in[6], int nt, const double *t,
+                       double rtol_ln, double atol_ln, int64_t max_steps, double *result,
+                       oracle_stats *stats, double *tape, int64_t tape_steps)
+{
+    return dop853_run(p, y0_in, nt, t, rtol_ln, atol_ln, max_steps, result, stats, tape,
+                      tape_steps);
 }
 
 /* ------------------------------------------------------------------ */

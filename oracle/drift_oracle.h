@@ -87,6 +87,14 @@ int oracle_dop853(const oracle_potential *p, const double y0[6], int nt, const d
                   double rtol_ln, double atol_ln, int64_t max_steps, double *result,
                   oracle_stats *stats);
 
+/* oracle_dop853 that also records its accepted steps: row j of `tape`
+ * (8 doubles) is (t_old, h, y_old[6]) of accepted step j, for the first
+ * tape_steps accepted steps (stats->accepted counts all of them).  The same
+ * record the device integrator writes for the adjoint pass. */
+int oracle_dop853_tape(const oracle_potential *p, const double y0[6], int nt, const double *t,
+                       double rtol_ln, double atol_ln, int64_t max_steps, double *result,
+                       oracle_stats *stats, double *tape, int64_t tape_steps);
+
 /* Batch driver: restates src/dispatch/cpu.rs:53-89 (per-particle loop and
  * time-major scatter into (nt, n, 6)).  Either `ts` (shared grid of nt times)
  * or `t_end` (per-particle end times on the grid t0..t_end[i] with nt points,

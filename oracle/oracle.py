@@ -92,6 +92,11 @@ def lib() -> ctypes.CDLL:
             ctypes.POINTER(Potential), dp, ctypes.c_int, dp, ctypes.c_double,
             ctypes.c_double, ctypes.c_int64, dp, ctypes.POINTER(Stats),
         ]
+        _lib.oracle_dop853_tape.restype = ctypes.c_int
+        _lib.oracle_dop853_tape.argtypes = [
+            ctypes.POINTER(Potential), dp, ctypes.c_int, dp, ctypes.c_double,
+            ctypes.c_double, ctypes.c_int64, dp, ctypes.POINTER(Stats), dp, ctypes.c_int64,
+        ]
         _lib.oracle_integrate_batch.restype = ctypes.c_int64
         _lib.oracle_integrate_batch.argtypes = [
             ctypes.c_int, ctypes.POINTER(Potential), ctypes.c_int64, dp, ctypes.c_int, dp,
@@ -152,6 +157,20 @@ def dop853(pot: Potential, y0, t, rtol_ln: float, atol_ln: float, max_steps: int
     status = lib().oracle_dop853(ctypes.byref(pot), _dptr(y0), len(t), _dptr(t), rtol_ln,
                                  atol_ln, max_steps, _dptr(res), ctypes.byref(st))
     return res, status, st
+
+
+def dop853_tape(pot: Potential, y0, t, rtol_ln: float, atol_ln: float, tape_steps: int = 100000):
+    """DOP853 with its accepted steps recorded: returns (result, status, stats,
+    tape (accepted, 8) of (t_old, h, y_old[6]))."""
+    y0 = np.ascontiguousarray(y0, dtype=np.float64)
+    t = np.ascontiguousarray(t, dtype=np.float64)
+    res = np.zeros((len(t), 6))
+    tape = np.zeros((tape_steps, 8))
+    st = Stats()
+    status = lib().oracle_dop853_tape(ctypes.byref(pot), _dptr(y0), len(t), _dptr(t), rtol_ln,
+                                      atol_ln, 0, _dptr(res), ctypes.byref(st), _dptr(tape),
+                                      tape_steps)
+    return res, status, st, tape[: min(st.accepted, tape_steps)].copy()
 
 
 def integrate_batch(method: int, pot: Potential, y0: np.ndarray, *, ts=None, t0: float = 0.0,

@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_messages():
     lib = capi.lib()
-    assert lib.drift_abi_version() == 1
+    assert lib.drift_abi_version() == 2
     assert lib.drift_result_string(0) == b"success"
     assert lib.drift_result_string(1) == b"invalid argument"
 
@@ -42,7 +42,9 @@ def test_struct_layout_matches_header(tmp_path):
     import subprocess
 
     lines = []
-    for struct_name, cls in (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch)):
+    structs = (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch),
+               ("drift_adjoint_launch", capi.DriftAdjointLaunch))
+    for struct_name, cls in structs:
         lines.append(f'printf("{struct_name} %zu\\n", sizeof({struct_name}));')
         for field, _ in cls._fields_:
             lines.append(f'printf("{struct_name}.{field} %zu\\n", offsetof({struct_name}, {field}));')
@@ -53,7 +55,7 @@ def test_struct_layout_matches_header(tmp_path):
     subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
     got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
                                                          check=True).stdout.splitlines())
-    for struct_name, cls in (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch)):
+    for struct_name, cls in structs:
         assert int(got[struct_name]) == ctypes.sizeof(cls)
         for field, _ in cls._fields_:
             assert int(got[f"{struct_name}.{field}"]) == getattr(cls, field).offset, field
@@ -72,6 +74,10 @@ def test_struct_layout_matches_header(tmp_path):
         (lambda L: setattr(L, "rtol_ln", float("nan")), "tolerances"),
         (lambda L: setattr(L, "ts", None), "either ts or t_end"),
         (lambda L: setattr(L, "y0", None), "y0 is NULL"),
+        (lambda L: (setattr(L, "tape", 4096), setattr(L, "tape_steps", 8), setattr(L, "method", 0)),
+         "recorded by DOP853 only"),
+        (lambda L: (setattr(L, "tape", 4096), setattr(L, "tape_steps", 0)), "tape_steps"),
+        (lambda L: (setattr(L, "tape", 4104), setattr(L, "tape_steps", 8)), "16-byte aligned"),
     ],
 )
 def test_invalid_launches_are_rejected_before_any_device_work(mutate, message):
@@ -105,3 +111,32 @@ def test_bovy_descriptor_normalises_bulge():
     assert abs(p.bulge_gamma_s - gs) < 1e-15 * gs
     # F_r(1) = -k gamma(s, 1/rc^2) = -0.05
     assert abs(p.bulge_k * gammainc(s, 1.0 / (1.9 / 8.0) ** 2) * gs - 0.05) < 1e-15
+
+
+def test_host_entry_point_rejects_a_step_tape():
+    y0 = np.zeros((4, 6))
+    ts = np.linspace(0.0, 1.0, 3)
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 4, 3, rtol=1e-10, atol=1e-10)
+    L.y0, L.ts = y0.ctypes.data, ts.ctypes.data
+    L.tape, L.tape_steps = 4096, 8
+    assert capi.lib().drift_integrate_host(ctypes.byref(L)) == 1
+    assert "device" in capi.lib().drift_last_error().decode()
+
+
+@pytest.mark.parametrize(
+    "mutate, message",
+    [
+        (lambda A: setattr(A, "method", 0), "supports DOP853"),
+        (lambda A: setattr(A, "tape", None), "required"),
+        (lambda A: setattr(A, "grad_out", None), "required"),
+        (lambda A: setattr(A, "nt", 1), "nt in"),
+        (lambda A: setattr(A.potential, "kind", 9), "unknown potential"),
+        (lambda A: setattr(A, "block_size", 256), "block_size"),
+    ],
+)
+def test_invalid_adjoint_launches_are_rejected(mutate, message):
+    A = capi.DriftAdjointLaunch(method=capi.DOP853, potential=capi.plummer(), n=4, nt=3, ts=4096,
+                                tape=4096, tape_steps=8, n_accepted=4096, grad_out=4096, grad_y0=4096)
+    mutate(A)
+    assert capi.lib().drift_integrate_adjoint(ctypes.byref(A), None) == 1
+    assert message in capi.lib().drift_last_error().decode()
