@@ -503,10 +503,16 @@ extern "C" int drift_integrate_adjoint(const drift_adjoint_launch *A, void *stre
     a.grad_params = A->grad_params;
     a.potential = A->potential;
     if (k == DRIFT_POT_BOVY) drift::fill_bulge_table(1.5 - 0.5 * A->potential.bulge_alpha, &a.bulge);
-    const int block = A->block_size ? A->block_size : drift::adjoint::ADJ_THREADS;
     int dev = 0, sms = 148;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaGetLastError();
+    // Default block: the largest of 128, 64, 32 threads that still gives
+    // every SM two blocks, so small particle counts spread over the GPU.
+    int block = A->block_size;
+    if (!block) {
+        block = drift::adjoint::ADJ_THREADS;
+        while (block > 32 && (A->n + block - 1) / block < 2 * (int64_t)sms) block /= 2;
+    }
     const int64_t blocks = std::min<int64_t>((A->n + block - 1) / block, (int64_t)sms * 64);
     cudaError_t e = drift::adjoint::launch(a, (int)blocks, block, static_cast<cudaStream_t>(stream));
     if (e != cudaSuccess)

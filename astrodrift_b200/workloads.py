@@ -86,3 +86,14 @@ def bovy_disc(n: int, seed: int = 3, radial_force=None) -> tuple[np.ndarray, np.
     y0 = np.stack([R * c, R * s, z, vR * c - vT * s, vR * s + vT * c, vz], axis=1)
     t_end = rng.uniform(10.0, 1000.0, n)
     return np.ascontiguousarray(y0), t_end
+
+
+def stream_progenitor(n: int, vc: float, seed: int = 5) -> tuple[np.ndarray, np.ndarray]:
+    """Configuration 5: a progenitor at R = 1.5, z = 0.2, phi = 0 moving with
+    v = (0, v_c(1.5), 0), and n particles offset from it by N(0, 0.002) in
+    position and N(0, 0.005) in velocity.  `vc` is the composite's circular
+    speed at R = 1.5.  Returns (progenitor (6,), particles (n, 6))."""
+    rng = np.random.default_rng(seed)
+    prog = np.array([1.5, 0.0, 0.2, 0.0, vc, 0.0])
+    y0 = prog[None, :] + np.hstack([rng.normal(0.0, 0.002, (n, 3)), rng.normal(0.0, 0.005, (n, 3))])
+    return prog, np.ascontiguousarray(y0)

@@ -54,6 +54,12 @@ FORCE_FLOPS = 10
 FLOPS_PER_ACCEPTED = FLOPS_ATTEMPT + FLOPS_ACCEPT_EXTRA + 15 * FORCE_FLOPS  # 2016
 FLOPS_PER_REJECTED = FLOPS_ATTEMPT + 11 * FORCE_FLOPS  # 1058
 FLOPS_PER_SAMPLE = 87
+# DRAM bytes (read + write) per particle of one launch of this workload,
+# from the ncu capture of 262,144 particles with the ordered schedule
+# (profiles/dop853_plummer_c2.txt, section 5: 1.696 GB read + 3.397 GB
+# written); traffic grows in proportion to the particles processed, so a
+# full launch is this times n.
+DRAM_BYTES_PER_PARTICLE = (1.696054272e9 + 3.397321984e9) / 262144
 
 
 def _dist():
@@ -386,6 +392,288 @@ def run_serving(args) -> None:
         s_.free()
 
 
+def run_config(args) -> None:
+    """The other two single-GPU configurations.
+
+    kepler -- configuration 1: 1,024 particles in the galpy-cylindrical Kepler
+              force (amp 1), DOPR54 at rtol = atol = 1e-10, ts = (0, 20 pi, 1001).
+    bovy   -- configuration 3: Bovy composite, R log-uniform on [0.05, 20],
+              per-particle t_end ~ U[10, 1000] with 101 outputs each, DOP853 at
+              1e-10.  The full configuration has 2^22 particles; the default
+              is its first 2^18 (--particles 4194304 runs it whole).  The
+              chosen schedule is timed beside one plain-schedule pass of the
+              same particles (the plain-launch baseline).
+    The line reports accepted steps/s, the energy drift |E(end)/E(0) - 1|
+    over all particles, and the plain-launch ratio.
+    """
+    import torch
+
+    from astrodrift_b200 import capi
+    from astrodrift_b200.energy import drift_summary
+    from astrodrift_b200.workloads import bovy_disc, kepler_disc
+
+    world, rank, local = _dist()
+    if args.workload == "kepler" and rank != 0:
+        return  # configuration 1 is one small batch: rank 0 alone
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    dist = None
+    if args.workload == "bovy" and world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    precision = capi.EXACT if args.precision == "exact" else capi.FMA
+    schedule = {"plain": capi.PLAIN, "persistent": capi.PERSISTENT, "ordered": capi.ORDERED}[args.schedule]
+    shard = None
+    if args.workload == "kepler":
+        pot, method, tol = capi.kepler(1.0), capi.DOPR54, 1e-10
+        n = 1024 if args.particles == N_PARTICLES else args.particles
+        y0 = kepler_disc(n, seed=1)
+        ts, t_end, nt = np.linspace(0.0, 20.0 * np.pi, 1001), None, 1001
+        name, full = "kepler-dopr54", 1024
+    else:
+        pot, method, tol = capi.bovy(), capi.DOP853, 1e-10
+        full = 1 << 22
+        n = (1 << 18) if args.particles == N_PARTICLES else args.particles
+        fr_pot = capi.bovy()
+
+        def radial_force(R):
+            xyz = torch.zeros((len(R), 3), dtype=torch.float64, device=dev)
+            xyz[:, 0] = torch.from_numpy(np.asarray(R, dtype=np.float64))
+            acc = torch.empty_like(xyz)
+            capi.force_device(fr_pot, len(R), xyz.data_ptr(), acc.data_ptr())
+            torch.cuda.synchronize()
+            return acc[:, 0].cpu().numpy()
+
+        y0_all, te_all = bovy_disc(full, seed=3, radial_force=radial_force)
+        y0, t_end = y0_all[:n], te_all[:n]
+        if dist:
+            # strong scaling: cost-balanced contiguous shards of the same particles
+            from astrodrift_b200.sharding import balanced_ranges, orbit_cost
+
+            xyz = torch.from_numpy(np.ascontiguousarray(y0[:, :3])).to(dev)
+            acc = torch.empty_like(xyz)
+            capi.force_device(fr_pot, n, xyz.data_ptr(), acc.data_ptr())
+            torch.cuda.synchronize()
+            lo, hi = balanced_ranges(orbit_cost(y0, t_end, acc.cpu().numpy()), world)[rank]
+            y0, t_end, shard = y0[lo:hi], t_end[lo:hi], (lo, hi)
+        ts, nt = None, 101
+        name = "bovy-uneven-dop853"
+    y0_d = torch.from_numpy(np.ascontiguousarray(y0)).to(dev)
+    grid_d = torch.from_numpy(ts if ts is not None else np.ascontiguousarray(t_end)).to(dev)
+    out_d = torch.empty((nt, n, 6), dtype=torch.float64, device=dev)
+    acc_d = torch.zeros(n, dtype=torch.int32, device=dev)
+    rej_d = torch.zeros(n, dtype=torch.int32, device=dev)
+    st_d = torch.zeros(n, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def make(sched):
+        L = capi.make_launch(method, pot, n, nt, rtol=tol, atol=tol, precision=precision, schedule=sched,
+                             block_size=args.block)
+        L.y0, L.out = y0_d.data_ptr(), out_d.data_ptr()
+        if ts is not None:
+            L.ts = grid_d.data_ptr()
+        else:
+            L.t_end = grid_d.data_ptr()
+        L.n_accepted, L.n_rejected, L.status = acc_d.data_ptr(), rej_d.data_ptr(), st_d.data_ptr()
+        ws = torch.zeros(max(capi.query_workspace(L), 8), dtype=torch.uint8, device=dev)
+        L.workspace, L.workspace_bytes = ws.data_ptr(), ws.numel()
+        return L, ws
+
+    def timed(L, steps):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+        for a_, b_ in ev:
+            a_.record(stream)
+            capi.integrate_device(L, stream.cuda_stream)
+            b_.record(stream)
+        torch.cuda.synchronize()
+        return [a_.elapsed_time(b_) / 1e3 for a_, b_ in ev]
+
+    n_all = n
+    n = len(y0)
+    L, ws = make(schedule)
+    timed(L, max(args.warmup, 3))
+    gpu_id = str(torch.cuda.get_device_properties(dev).uuid)
+    gpu_id = gpu_id if gpu_id.startswith("GPU-") else f"GPU-{gpu_id}"
+    if dist:
+        dist.barrier()
+    with ClockSampler(gpu_id) as clocks:
+        secs = timed(L, args.steps)
+    status = st_d.cpu().numpy()
+    accepted = int(acc_d.cpu().numpy().astype(np.int64).sum())
+    rejected = int(rej_d.cpu().numpy().astype(np.int64).sum())
+    acc_per = acc_d.cpu().numpy()
+    out_first = out_d[0].cpu().numpy()
+    last_idx = nt - 1
+    out_last = out_d[last_idx].cpu().numpy()
+    mean_s = statistics.mean(secs)
+    if dist:
+        from astrodrift_b200.sharding import reduce_max, reduce_sum
+
+        mean_s = reduce_max(mean_s, dist, dev)
+        accepted = int(reduce_sum(accepted, dist, dev))
+        rejected = int(reduce_sum(rejected, dist, dev))
+        dist.barrier()
+        dist.destroy_process_group()
+        if rank != 0:
+            return
+    value = accepted / mean_s
+    plain = None
+    if schedule != capi.PLAIN and not args.no_plain and not dist:
+        Lp, wsp = make(capi.PLAIN)
+        psecs = timed(Lp, 1)
+        plain = {"value": accepted / psecs[0], "seconds": psecs[0], "speedup": psecs[0] / statistics.mean(secs),
+                 "bitwise_equal_trajectory": bool(np.array_equal(out_d[last_idx].cpu().numpy(), out_last))}
+    line = {
+        "metric": "accepted steps/s",
+        "value": value,
+        "unit": "accepted steps/s",
+        "n_gpus": world if dist else 1,
+        "steps": args.steps,
+        "warmup": max(args.warmup, 3),
+        "ms_per_step": 1e3 * mean_s,
+        "higher_is_better": True,
+        "scaling": "strong" if dist else "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded, configuration generator)",
+        "config": {"workload": name if n_all == full else f"{name} (first {n_all} of {full})",
+                   "particles": n_all, "rank0_shard": shard,
+                   "nt": nt, "rtol": tol, "method": "DOP853" if method == capi.DOP853 else "DOPR54",
+                   "precision": args.precision, "schedule": args.schedule,
+                   "l2": "outputs written once per pass; inputs re-read each pass"},
+        "accepted_steps_per_pass": accepted,
+        "rejected_steps_per_pass": rejected,
+        "steps_per_particle": {"median": float(np.median(acc_per)), "max": int(acc_per.max()),
+                               "min": int(acc_per.min())},
+        "particles_not_ok": int((status != 0).sum()),
+        "energy_drift": drift_summary(pot, out_first, out_last),  # rank 0's particles
+        "plain_launch": plain,
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_gradient(args) -> None:
+    """Stream-fitting gradient: 65,536 particles sprayed around a progenitor in
+    the Bovy composite, DOP853 at rtol = atol = 1e-10 to t = 50; loss
+    sum_i |x_i(50) - track(s_i)|^2 against a cubic-spline track through 32
+    seeded points (s_i: the closest point of a dense sampling of the track to
+    the particle's first-pass position, then held fixed).  One step = the
+    taped forward integration, the loss and the adjoint pass, giving the
+    gradient with respect to all 6-D initial conditions and the potential's
+    parameters (MN amp, MN a and NFW a among them).  The metric counts the
+    forward pass's accepted steps per second of the whole step.
+    """
+    import torch
+    from scipy.interpolate import CubicSpline
+
+    from astrodrift_b200 import adjoint, capi
+    from astrodrift_b200.workloads import stream_progenitor
+
+    world, rank, local = _dist()
+    if rank != 0:
+        return
+    torch.cuda.set_device(local)
+    dev = torch.device(f"cuda:{local}")
+    n = 65536 if args.particles == N_PARTICLES else args.particles
+    pot = capi.bovy()
+    # circular speed at R = 1.5 from the composite's force
+    xyz = torch.tensor([[1.5, 0.0, 0.0]], dtype=torch.float64, device=dev)
+    acc = torch.empty_like(xyz)
+    capi.force_device(pot, 1, xyz.data_ptr(), acc.data_ptr())
+    torch.cuda.synchronize()
+    vc = float(np.sqrt(1.5 * abs(float(acc[0, 0]))))
+    prog, y0 = stream_progenitor(n, vc, seed=5)
+    ts = np.array([0.0, 50.0])
+    rtol = 1e-10
+    # target track: the progenitor's positions at 32 times in [45, 55] plus
+    # seeded N(0, 0.01) offsets
+    rng = np.random.default_rng(6)
+    grid = np.concatenate([[0.0], np.linspace(45.0, 55.0, 32)])
+    pts = capi.integrate_host(capi.DOP853, pot, prog[None, :], ts=grid, rtol=rtol, atol=rtol)["out"][1:, 0, :3]
+    pts = pts + rng.normal(0.0, 0.01, pts.shape)
+    spline = CubicSpline(np.linspace(0.0, 1.0, 32), pts)
+    dense = spline(np.linspace(0.0, 1.0, 4096))
+    y0_d = torch.tensor(y0, device=dev)
+    params0 = adjoint.params_of(pot)
+    first = adjoint.trajectory(y0_d, pot, ts=ts, rtol=rtol, atol=rtol)
+    x50 = first[-1, :, :3].cpu().numpy()
+    # closest dense-track point of each particle (chunked to bound memory)
+    target = np.empty_like(x50)
+    for i in range(0, n, 4096):
+        d = ((x50[i:i + 4096, None, :] - dense[None, :, :]) ** 2).sum(-1)
+        target[i:i + 4096] = dense[d.argmin(axis=1)]
+    target_d = torch.tensor(target, device=dev)
+    # tape sized once from an untaped pass
+    acc_d = torch.zeros(n, dtype=torch.int32, device=dev)
+    L = capi.make_launch(capi.DOP853, pot, n, 2, rtol=rtol, atol=rtol, precision=capi.FMA,
+                         schedule=capi.ORDERED)
+    ts_d = torch.tensor(ts, device=dev)
+    L.y0, L.ts, L.n_accepted = y0_d.data_ptr(), ts_d.data_ptr(), acc_d.data_ptr()
+    ws = torch.zeros(capi.query_workspace(L), dtype=torch.uint8, device=dev)
+    L.workspace, L.workspace_bytes = ws.data_ptr(), ws.numel()
+    capi.integrate_device(L, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    steps_acc = int(acc_d.to(torch.int64).sum())
+    tape_steps = int(acc_d.max())
+
+    def step():
+        y = y0_d.clone().requires_grad_(True)
+        p = torch.tensor(params0, dtype=torch.float64, requires_grad=True)
+        out = adjoint.trajectory(y, pot, params=p, ts=ts, rtol=rtol, atol=rtol, tape_steps=tape_steps)
+        loss = ((out[-1, :, :3] - target_d) ** 2).sum()
+        ev = torch.cuda.Event(enable_timing=True)
+        ev.record()
+        loss.backward()
+        return loss, y, p, ev
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    back_ms = []
+    with ClockSampler(str(local)) as clocks:
+        s.record()
+        for _ in range(args.steps):
+            loss, y, p, ev = step()
+            ev_end = torch.cuda.Event(enable_timing=True)
+            ev_end.record()
+            back_ms.append((ev, ev_end))
+        e.record()
+        torch.cuda.synchronize()
+    ms = s.elapsed_time(e) / args.steps
+    back = statistics.median(a.elapsed_time(b) for a, b in back_ms)
+    names = adjoint.PARAM_NAMES[pot.kind]
+    line = {
+        "metric": "accepted steps/s (forward + adjoint gradient)",
+        "value": steps_acc / (ms * 1e-3),
+        "unit": "accepted steps/s",
+        "n_gpus": 1,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded progenitor spray, seeded track)",
+        "config": {"workload": "stream-gradient", "particles": n, "potential": "bovy", "method": "DOP853",
+                   "rtol": rtol, "t_end": 50.0, "accepted_steps": steps_acc, "tape_rows": tape_steps,
+                   "tape_bytes": n * tape_steps * 64, "l2": "inputs reused; trajectory is 2 samples"},
+        "backward_ms": back,
+        "forward_ms": ms - back,
+        "loss": float(loss),
+        "grad_norm_y0": float(y.grad.norm()),
+        "grad_params": {k: float(v) for k, v in zip(names, p.grad.tolist())},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -402,8 +690,12 @@ def main() -> None:
     ap.add_argument("--no-peak", action="store_true", help="skip the FP64 peak probe (profiling runs)")
     ap.add_argument("--particles", type=int, default=N_PARTICLES,
                     help="particles per GPU (default: the workload's 2^20; smaller for ncu captures)")
-    ap.add_argument("--workload", default="plummer", choices=["plummer", "serving"],
-                    help="plummer: the benchmark configuration; serving: a Poisson request stream")
+    ap.add_argument("--workload", default="plummer",
+                    choices=["plummer", "kepler", "bovy", "serving", "stream-gradient"],
+                    help="plummer: the benchmark configuration; kepler / bovy: the other single-GPU "
+                         "configurations; serving: a Poisson request stream; stream-gradient: forward + "
+                         "adjoint gradient of a stream-track loss")
+    ap.add_argument("--no-plain", action="store_true", help="kepler/bovy: skip the plain-launch pass")
     ap.add_argument("--requests", type=int, default=32, help="serving: requests in the stream")
     ap.add_argument("--loads", default="0.5,0.8",
                     help="serving: offered loads (fractions of the saturated capacity) for latency")
@@ -418,6 +710,12 @@ def main() -> None:
         return
     if args.workload == "serving":
         run_serving(args)
+        return
+    if args.workload == "stream-gradient":
+        run_gradient(args)
+        return
+    if args.workload in ("kepler", "bovy"):
+        run_config(args)
         return
 
     import torch
@@ -491,14 +789,15 @@ def main() -> None:
     rejected = int(rej_d.cpu().numpy().astype(np.int64).sum())
     if (status != 0).any():
         raise RuntimeError(f"{int((status != 0).sum())} particles did not finish")
+    from astrodrift_b200.energy import drift_summary
+
+    e_drift = drift_summary(capi.plummer(1.0, 1.0), out_d[0].cpu().numpy(), out_d[-1].cpu().numpy())
 
     if dist:
-        t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
-        a = torch.tensor([accepted], dtype=torch.float64, device=dev)
-        dist.all_reduce(a, op=dist.ReduceOp.SUM)
-        accepted_all = float(a.item())
+        from astrodrift_b200.sharding import reduce_max, reduce_sum
+
+        elapsed = reduce_max(elapsed, dist, dev)
+        accepted_all = reduce_sum(accepted, dist, dev)
     else:
         accepted_all = float(accepted)
     value = accepted_all * args.steps / elapsed
@@ -535,9 +834,7 @@ def main() -> None:
             e2e_step()
         e2e_elapsed = time.perf_counter() - t0
         if dist:
-            t = torch.tensor([e2e_elapsed], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_elapsed = float(t.item())
+            e2e_elapsed = reduce_max(e2e_elapsed, dist, dev)
         e2e_value = accepted_all * args.e2e_steps / e2e_elapsed
         e2e_ok = bool(np.array_equal(out_pinned[-1], out_d[-1].cpu().numpy()))
         del y0_pinned, out_pinned
@@ -582,7 +879,10 @@ def main() -> None:
             "rejected_steps_per_pass": rejected,
             "gpu_launches": args.steps,
             "roofline": {"bound": "fp64", "achieved": achieved_tflops, "peak": fp64_peak,
-                         "unit": "TFLOP/s", "frac": achieved_tflops / fp64_peak, "traffic": None,
+                         "unit": "TFLOP/s", "frac": achieved_tflops / fp64_peak,
+                         "traffic": DRAM_BYTES_PER_PARTICLE * n,
+                         "traffic_source": "ncu dram__bytes_read+write at 262,144 particles, scaled by "
+                                           "particles (profiles/dop853_plummer_c2.txt, section 5)",
                          "peak_source": "FP64 DGEMM (torch.matmul float64 8192^3, best of 5) "
                                         "measured in this run; MEASURED_PEAKS.json has no FP64 figure",
                          "flops_per_launch": flops,
@@ -593,6 +893,7 @@ def main() -> None:
                              "peak": hbm_peak, "unit": "GB/s",
                              "frac": bytes_alg / mean_launch / 1e9 / hbm_peak, "peak_source": hbm_src},
             "kernel_ms_mean": 1e3 * mean_launch,
+            "energy_drift": e_drift,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "accepted steps/s",
                     "h2d_bytes_per_step": int(y0.nbytes + ts.nbytes),
