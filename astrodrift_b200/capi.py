@@ -17,7 +17,8 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdrift_b200.so"
 
 DOPR54, DOP853 = 0, 1
-POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN = 0, 1, 2, 3
+POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN, POT_MODEL = 0, 1, 2, 3, 4
+MAX_COMPONENTS = 11
 EXACT, FMA = 0, 1
 PLAIN, PERSISTENT, ORDERED = 0, 1, 2
 INITIAL_STEP_SENTINEL = -9999.99
@@ -47,6 +48,8 @@ EXPORTED = (
     "drift_server_stats_get",
     "drift_server_destroy",
     "drift_integrate_adjoint",
+    "drift_origin_table",
+    "drift_force_model_eval",
 )
 
 
@@ -65,6 +68,31 @@ class DriftPotential(ctypes.Structure):
         ("bulge_rc", ctypes.c_double),
         ("bulge_k", ctypes.c_double),
         ("bulge_gamma_s", ctypes.c_double),
+    ]
+
+
+class DriftSourceGroup(ctypes.Structure):
+    _fields_ = [
+        ("kind", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("amp", ctypes.c_double),
+        ("b", ctypes.c_double),
+        ("first", ctypes.c_int64),
+        ("count", ctypes.c_int64),
+    ]
+
+
+class DriftForceModel(ctypes.Structure):
+    _fields_ = [
+        ("n_static", ctypes.c_int32),
+        ("n_groups", ctypes.c_int32),
+        ("statics", DriftPotential * MAX_COMPONENTS),
+        ("groups", DriftSourceGroup * MAX_COMPONENTS),
+        ("n_sources", ctypes.c_int64),
+        ("n_segments", ctypes.c_int64),
+        ("t0", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("origins", ctypes.c_void_p),
     ]
 
 
@@ -96,6 +124,7 @@ class DriftLaunch(ctypes.Structure):
         ("workspace_bytes", ctypes.c_size_t),
         ("tape", ctypes.c_void_p),
         ("tape_steps", ctypes.c_int64),
+        ("force_model", ctypes.POINTER(DriftForceModel)),
     ]
 
 
@@ -146,6 +175,11 @@ def lib() -> ctypes.CDLL:
         L.drift_integrate_noalloc.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
         L.drift_integrate_batch.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_int32, ctypes.c_void_p]
         L.drift_integrate_adjoint.argtypes = [ctypes.POINTER(DriftAdjointLaunch), ctypes.c_void_p]
+        L.drift_origin_table.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_int64,
+                                         ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
+                                         ctypes.c_void_p]
+        L.drift_force_model_eval.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_double,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
     return _lib
 
@@ -185,6 +219,45 @@ def bovy(**overrides) -> DriftPotential:
     return pot
 
 
+def force_model(statics=(), groups=(), *, origins=None, n_sources=0, n_segments=0, t0=0.0,
+                dt=1.0) -> DriftForceModel:
+    """A summed force: `statics` (DriftPotentials, kinds 0..3) then `groups`,
+    each (kind, amp, b, first, count) with kind POT_KEPLER_CARTESIAN or
+    POT_PLUMMER; `origins` is the address of the (n_segments, n_sources, 18)
+    origin table (device for device entry points, host for integrate_host)."""
+    m = DriftForceModel()
+    if len(statics) > MAX_COMPONENTS or len(groups) > MAX_COMPONENTS:
+        raise ValueError(f"at most {MAX_COMPONENTS} stationary parts and source groups")
+    m.n_static = len(statics)
+    for i, p in enumerate(statics):
+        m.statics[i] = p
+    m.n_groups = len(groups)
+    for i, (kind, amp, b, first, count) in enumerate(groups):
+        m.groups[i] = DriftSourceGroup(kind=kind, amp=amp, b=b, first=first, count=count)
+    m.origins = origins
+    m.n_sources, m.n_segments, m.t0, m.dt = n_sources, n_segments, t0, dt
+    return m
+
+
+def model_potential() -> DriftPotential:
+    """The potential descriptor that selects drift_launch.force_model."""
+    return DriftPotential(kind=POT_MODEL)
+
+
+def origin_table_device(source_model: DriftForceModel, n_sources: int, nt: int, t0: float, dt: float,
+                        traj_ptr: int, origins_ptr: int, stream: int = 0) -> None:
+    check(lib().drift_origin_table(ctypes.byref(source_model), n_sources, nt, t0, dt,
+                                   ctypes.c_void_p(traj_ptr), ctypes.c_void_p(origins_ptr),
+                                   ctypes.c_void_p(stream)), "drift_origin_table")
+
+
+def force_model_eval_device(model: DriftForceModel, n: int, t: float, xyz_ptr: int, acc_ptr: int,
+                            stream: int = 0) -> None:
+    check(lib().drift_force_model_eval(ctypes.byref(model), n, t, ctypes.c_void_p(xyz_ptr),
+                                       ctypes.c_void_p(acc_ptr), ctypes.c_void_p(stream)),
+          "drift_force_model_eval")
+
+
 def _ptr(a) -> int | None:
     return None if a is None else a.ctypes.data
 
@@ -207,8 +280,11 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
                    t0: float = 0.0, rtol: float = 1e-12, atol: float = 1e-12,
                    precision: int = EXACT, schedule: int = PERSISTENT, block_size: int = 0,
                    dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
-                   timeout_s: float = 0.0, want_out: bool = True, out=None) -> dict:
-    """drift_integrate_host: host arrays in, host arrays out."""
+                   timeout_s: float = 0.0, want_out: bool = True, out=None,
+                   model: DriftForceModel | None = None) -> dict:
+    """drift_integrate_host: host arrays in, host arrays out.  With `model`
+    (whose origin table is a host array), `pot` is ignored and the stage
+    integrates in the summed force."""
     y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
     n = y0.shape[0]
     if ts is not None:
@@ -220,6 +296,9 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
     L = make_launch(method, pot, n, nt, rtol=rtol, atol=atol, precision=precision,
                     schedule=schedule, block_size=block_size, dt_one=dt_one,
                     max_steps=max_steps, timeout_s=timeout_s, t0=t0)
+    if model is not None:
+        L.potential = model_potential()
+        L.force_model = ctypes.pointer(model)
     if want_out and out is None:
         out = np.empty((nt, n, 6))
     res = dict(

@@ -99,7 +99,7 @@ struct DeviceContext {
     std::mutex mu;  // serialises host-buffer calls that share the buffers below
     cudaStream_t streams[2] = {nullptr, nullptr};
     cudaEvent_t done[2] = {nullptr, nullptr};
-    DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor;
+    DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor, origins;
     HostBuf stage[2];
 };
 
@@ -132,6 +132,57 @@ int current_context(DeviceContext **out)
 
 bool is_finite_value(double v) { return std::isfinite(v); }
 
+// A force model's own consistency (its pointers are checked by the caller).
+int validate_model(const drift_force_model *m)
+{
+    if (!m) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "potential kind DRIFT_POT_MODEL needs force_model");
+    if (m->n_static < 0 || m->n_static > DRIFT_MAX_COMPONENTS || m->n_groups < 0 ||
+        m->n_groups > DRIFT_MAX_COMPONENTS)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "a force model has at most " + std::to_string(DRIFT_MAX_COMPONENTS) +
+                        " stationary parts and source groups");
+    double alpha = 0.0;
+    bool bovy = false;
+    for (int i = 0; i < m->n_static; i++) {
+        const int k = m->statics[i].kind;
+        if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown kind of a force model's stationary part");
+        if (k == DRIFT_POT_BOVY) {
+            if (bovy && m->statics[i].bulge_alpha != alpha)
+                return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the Bovy parts of a force model must share bulge_alpha");
+            bovy = true;
+            alpha = m->statics[i].bulge_alpha;
+        }
+    }
+    int64_t need = 0;
+    for (int g = 0; g < m->n_groups; g++) {
+        const drift_source_group &G = m->groups[g];
+        if (G.kind != DRIFT_POT_KEPLER_CARTESIAN && G.kind != DRIFT_POT_PLUMMER)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                        "only Kepler and Plummer potentials can currently be attached to particles");
+        if (G.first < 0 || G.count < 0) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "negative source range");
+        need = std::max(need, G.first + G.count);
+    }
+    if (m->n_groups > 0) {
+        if (need > m->n_sources) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "source ranges exceed n_sources");
+        if (m->n_segments < 1 || !m->origins)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "moving sources need an origin table (n_segments >= 1)");
+        if (!is_finite_value(m->t0) || !is_finite_value(m->dt) || m->dt == 0.0)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the origin table needs finite t0 and a nonzero dt");
+    }
+    return DRIFT_SUCCESS;
+}
+
+// The bulge table a model needs (from its first Bovy part), or none.
+void fill_model_bulge(const drift_force_model &m, drift::BulgeTable *t)
+{
+    for (int i = 0; i < m.n_static; i++)
+        if (m.statics[i].kind == DRIFT_POT_BOVY) {
+            drift::fill_bulge_table(1.5 - 0.5 * m.statics[i].bulge_alpha, t);
+            return;
+        }
+}
+
 int validate(const drift_launch *L, bool device_pointers)
 {
     if (!L) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "launch is NULL");
@@ -149,8 +200,16 @@ int validate(const drift_launch *L, bool device_pointers)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT,
                     "block_size must be 0 or a multiple of 32 in [32, " + std::to_string(max_block) + "]");
     const int k = L->potential.kind;
-    if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
+    if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_MODEL)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown potential kind");
+    if (k == DRIFT_POT_MODEL) {
+        int rc = validate_model(L->force_model);
+        if (rc) return rc;
+        if (L->force_model->n_groups > 0 && device_pointers &&
+            reinterpret_cast<uintptr_t>(L->force_model->origins) % 8)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the origin table must be 8-byte aligned");
+        if (L->tape) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the step tape supports single potentials");
+    }
     if (L->n < 1) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "n must be >= 1");
     if (L->n > (int64_t(1) << 40)) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "n is too large");
     if (L->nt < 2 || L->nt > INT32_MAX - 1)
@@ -215,6 +274,10 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
+    if (L->potential.kind == DRIFT_POT_MODEL) {
+        a.model = *L->force_model;
+        fill_model_bulge(a.model, &a.bulge);
+    }
     return a;
 }
 
@@ -580,6 +643,49 @@ int drift_force(const drift_potential *potential, int64_t n, const double *xyz, 
     return DRIFT_SUCCESS;
 }
 
+int drift_force_model_eval(const drift_force_model *model, int64_t n, double t, const double *xyz,
+                           double *acc, void *stream)
+{
+    if (!xyz || !acc || n < 0)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_force_model_eval: NULL pointer or negative n");
+    int rc = validate_model(model);
+    if (rc) return rc;
+    if (n == 0) return DRIFT_SUCCESS;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    int64_t blocks = std::min<int64_t>((n + 255) / 256, (int64_t)ctx->sm_count * 8);
+    drift::BulgeTable table;
+    std::memset(&table, 0, sizeof(table));
+    fill_model_bulge(*model, &table);
+    DRIFT_CUDA_TRY(drift::model_force_exact(*model, table, t, n, xyz, acc, (int)blocks,
+                                            static_cast<cudaStream_t>(stream)),
+                   "model force kernel launch");
+    return DRIFT_SUCCESS;
+}
+
+int drift_origin_table(const drift_force_model *source_model, int64_t n_sources, int64_t nt, double t0,
+                       double dt, const double *trajectory, double *origins, void *stream)
+{
+    if (!trajectory || !origins || n_sources < 1 || nt < 2)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "drift_origin_table: NULL pointer, n_sources < 1 or nt < 2");
+    if (!is_finite_value(t0) || !is_finite_value(dt) || dt == 0.0)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_origin_table: t0 finite and dt nonzero required");
+    int rc = validate_model(source_model);
+    if (rc) return rc;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    drift::BulgeTable table;
+    std::memset(&table, 0, sizeof(table));
+    fill_model_bulge(*source_model, &table);
+    DRIFT_CUDA_TRY(drift::origin_table_exact(*source_model, table, n_sources, nt, t0, dt, trajectory, origins,
+                                             static_cast<cudaStream_t>(stream)),
+                   "origin table kernel launch");
+    return DRIFT_SUCCESS;
+}
+
 int drift_host_alloc(size_t bytes, void **ptr)
 {
     if (!ptr) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "ptr is NULL");
@@ -645,6 +751,19 @@ int drift_integrate_host(const drift_launch *L)
             DRIFT_CUDA_TRY(ctx->stage[i].ensure(chunk * nt * row), "cudaMallocHost(stage)");
 
     cudaStream_t s0 = ctx->streams[0];
+    // A force model's origin table is a host array here: its device copy
+    // lives in the context.
+    drift_force_model model_dev{};
+    if (L->potential.kind == DRIFT_POT_MODEL) {
+        model_dev = *L->force_model;
+        if (model_dev.n_groups > 0) {
+            const size_t bytes = (size_t)model_dev.n_segments * model_dev.n_sources * 18 * sizeof(double);
+            DRIFT_CUDA_TRY(ctx->origins.ensure(bytes), "cudaMalloc(origins)");
+            DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->origins.ptr, model_dev.origins, bytes, cudaMemcpyHostToDevice, s0),
+                           "H2D origins");
+            model_dev.origins = ctx->origins.as<double>();
+        }
+    }
     DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->y0.ptr, L->y0, n * row, cudaMemcpyHostToDevice, s0), "H2D y0");
     DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->grid.ptr, L->ts ? (const void *)L->ts : (const void *)L->t_end,
                                    grid_bytes, cudaMemcpyHostToDevice, s0),
@@ -677,6 +796,7 @@ int drift_integrate_host(const drift_launch *L)
         }
         drift_launch sub = *L;
         sub.n = cn;
+        if (L->potential.kind == DRIFT_POT_MODEL) sub.force_model = &model_dev;
         sub.y0 = ctx->y0.as<double>() + c0 * 6;
         sub.ts = L->ts ? ctx->grid.as<double>() : nullptr;
         sub.t_end = L->ts ? nullptr : ctx->grid.as<double>() + c0;

@@ -22,6 +22,7 @@
 #pragma once
 
 #include "drift_common.cuh"
+#include "drift_composite.cuh"
 
 #ifndef DRIFT_EXACT_ARITH
 #define DRIFT_EXACT_ARITH 1
@@ -171,6 +172,20 @@ constexpr double ER9 = -0.3503288487499736816886487290;
 constexpr double ER10 = 0.3341791187130174790297318841;
 constexpr double ER11 = 0.8192320648511571246570742613e-1;
 constexpr double ER12 = -0.2235530786388629525884427845e-1;
+// Stage times c_i (the node of stage i is t + c_i h).
+constexpr double C2 = 0.526001519587677318785587544488e-1;
+constexpr double C3 = 0.789002279381515978178381316732e-1;
+constexpr double C4 = 0.118350341907227396726757197510;
+constexpr double C5 = 0.281649658092772603273242802490;
+constexpr double C6 = 0.333333333333333333333333333333;
+constexpr double C7 = 0.25;
+constexpr double C8 = 0.307692307692307692307692307692;
+constexpr double C9 = 0.651282051282051282051282051282;
+constexpr double C10 = 0.6;
+constexpr double C11 = 0.857142857142857142857142857142;
+constexpr double C14 = 0.1;
+constexpr double C15 = 0.2;
+constexpr double C16 = 0.777777777777777777777777777778;
 constexpr double SAFE = 0.9;
 constexpr double FACC1 = 1.0 / 0.333;
 constexpr double FACC2 = 1.0 / 6.0;
@@ -195,12 +210,13 @@ struct Dop853Lane {
     int32_t nonfinite_run;
     bool done;
 
-    __device__ __forceinline__ void rhs(const Pot &pot, const double *q, double *a) const
+    // a = f(t, q) = (v, F(t, x)); stationary potentials ignore t.
+    __device__ __forceinline__ void rhs(const Pot &pot, double t, const double *q, double *a) const
     {
         a[0] = q[3];
         a[1] = q[4];
         a[2] = q[5];
-        pot.force(q[0], q[1], q[2], a[3], a[4], a[5]);
+        force_at(pot, t, q[0], q[1], q[2], a[3], a[4], a[5]);
     }
 
     // dop853.rs:340-424: tolerances, Hairer's initial step, bookkeeping.
@@ -218,7 +234,7 @@ struct Dop853Lane {
         pos_neg = custom_sign(1.0, hmax);
         done = (grid.nt < 2);
 
-        rhs(pot, y, k1);
+        rhs(pot, t0, y, k1);
         double dnf = 0.0, dny = 0.0;
 #pragma unroll
         for (int i = 0; i < 6; i++) {
@@ -232,7 +248,7 @@ struct Dop853Lane {
         double k2[6], k3[6];
 #pragma unroll
         for (int i = 0; i < 6; i++) k3[i] = y[i] + hh * k1[i];
-        rhs(pot, k3, k2);
+        rhs(pot, t0 + hh, k3, k2);
         double der2 = 0.0;
 #pragma unroll
         for (int i = 0; i < 6; i++) {
@@ -265,45 +281,45 @@ struct Dop853Lane {
 
 #pragma unroll
         for (int i = 0; i < 6; i++) yy1[i] = y[i] + h * A21 * k1[i];
-        rhs(pot, yy1, k2);
+        rhs(pot, t_cur + C2 * h, yy1, k2);
 #pragma unroll
         for (int i = 0; i < 6; i++) yy1[i] = y[i] + h * (A31 * k1[i] + A32 * k2[i]);
-        rhs(pot, yy1, k3);
+        rhs(pot, t_cur + C3 * h, yy1, k3);
 #pragma unroll
         for (int i = 0; i < 6; i++) yy1[i] = y[i] + h * (A41 * k1[i] + A43 * k3[i]);
-        rhs(pot, yy1, k4);
+        rhs(pot, t_cur + C4 * h, yy1, k4);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A51 * k1[i] + A53 * k3[i] + A54 * k4[i]);
-        rhs(pot, yy1, k5);
+        rhs(pot, t_cur + C5 * h, yy1, k5);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A61 * k1[i] + A64 * k4[i] + A65 * k5[i]);
-        rhs(pot, yy1, k6);
+        rhs(pot, t_cur + C6 * h, yy1, k6);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A71 * k1[i] + A74 * k4[i] + A75 * k5[i] + A76 * k6[i]);
-        rhs(pot, yy1, k7);
+        rhs(pot, t_cur + C7 * h, yy1, k7);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] +
                      h * (A81 * k1[i] + A84 * k4[i] + A85 * k5[i] + A86 * k6[i] + A87 * k7[i]);
-        rhs(pot, yy1, k8);
+        rhs(pot, t_cur + C8 * h, yy1, k8);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A91 * k1[i] + A94 * k4[i] + A95 * k5[i] + A96 * k6[i] +
                                  A97 * k7[i] + A98 * k8[i]);
-        rhs(pot, yy1, k9);
+        rhs(pot, t_cur + C9 * h, yy1, k9);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A101 * k1[i] + A104 * k4[i] + A105 * k5[i] + A106 * k6[i] +
                                  A107 * k7[i] + A108 * k8[i] + A109 * k9[i]);
-        rhs(pot, yy1, k10);
+        rhs(pot, t_cur + C10 * h, yy1, k10);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A111 * k1[i] + A114 * k4[i] + A115 * k5[i] + A116 * k6[i] +
                                  A117 * k7[i] + A118 * k8[i] + A119 * k9[i] + A1110 * k10[i]);
-        rhs(pot, yy1, k2);
+        rhs(pot, t_cur + C11 * h, yy1, k2);
 #pragma unroll
         for (int i = 0; i < 6; i++)
             yy1[i] = y[i] + h * (A121 * k1[i] + A124 * k4[i] + A125 * k5[i] + A126 * k6[i] +
@@ -311,7 +327,7 @@ struct Dop853Lane {
                                  A1211 * k2[i]);
         const double t_old = t_cur;
         const double t_new = t_cur + h;
-        rhs(pot, yy1, k3);
+        rhs(pot, t_new, yy1, k3);
 
 #pragma unroll
         for (int i = 0; i < 6; i++) {
@@ -362,7 +378,7 @@ struct Dop853Lane {
                 row[2] = make_double2(y[2], y[3]);
                 row[3] = make_double2(y[4], y[5]);
             }
-            rhs(pot, k5, k4);  // FSAL: k4 = f(t_new, y_new)
+            rhs(pot, t_new, k5, k4);  // FSAL: k4 = f(t_new, y_new)
 
 #pragma unroll
             for (int i = 0; i < 6; i++) {
@@ -384,19 +400,19 @@ struct Dop853Lane {
                 yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] + A149 * k9[i] +
                                      A1410 * k10[i] + A1411 * k2[i] + A1412 * k3[i] +
                                      A1413 * k4[i]);
-            rhs(pot, yy1, k10);
+            rhs(pot, t_old + C14 * h, yy1, k10);
 #pragma unroll
             for (int i = 0; i < 6; i++)
                 yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] + A158 * k8[i] +
                                      A1511 * k2[i] + A1512 * k3[i] + A1513 * k4[i] +
                                      A1514 * k10[i]);
-            rhs(pot, yy1, k2);
+            rhs(pot, t_old + C15 * h, yy1, k2);
 #pragma unroll
             for (int i = 0; i < 6; i++)
                 yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] + A168 * k8[i] +
                                      A169 * k9[i] + A1613 * k4[i] + A1614 * k10[i] +
                                      A1615 * k2[i]);
-            rhs(pot, yy1, k3);
+            rhs(pot, t_old + C16 * h, yy1, k3);
 
             // rcont1..4 (dop853.rs:636-642) need only y, y_new, k1 and k4,
             // so they are formed here, after the extra stages.

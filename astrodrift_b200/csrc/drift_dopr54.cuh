@@ -24,6 +24,7 @@
 #pragma once
 
 #include "drift_common.cuh"
+#include "drift_composite.cuh"
 
 namespace drift {
 namespace dopr54c {
@@ -88,12 +89,13 @@ struct Dopr54Lane {
     int32_t err;   // galpy error code
     bool done;
 
-    __device__ __forceinline__ void rhs(const Pot &pot, const double *q, double *a) const
+    // a = f(t, q) = (v, F(t, x)); stationary potentials ignore t.
+    __device__ __forceinline__ void rhs(const Pot &pot, double t, const double *q, double *a) const
     {
         a[0] = q[3];
         a[1] = q[4];
         a[2] = q[5];
-        pot.force(q[0], q[1], q[2], a[3], a[4], a[5]);
+        force_at(pot, t, q[0], q[1], q[2], a[3], a[4], a[5]);
     }
 
     // 1 / (e^atol + e^rtol max_i |y_i|), the reciprocal of e^s.
@@ -109,32 +111,32 @@ struct Dopr54Lane {
     }
 
     // rk4_onestep (dopr54.rs:135-208): yn1 += RK4 increment of step dt.
-    __device__ __forceinline__ void rk4_onestep(const Pot &pot, const double *yv, double *yn1,
+    __device__ __forceinline__ void rk4_onestep(const Pot &pot, double tn, const double *yv, double *yn1,
                                                 double dtv) const
     {
         double a[6], ynk[6];
-        rhs(pot, yv, a);
+        rhs(pot, tn, yv, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) yn1[i] += dtv * a[i] / 6.0;
 #pragma unroll
         for (int i = 0; i < 6; i++) ynk[i] = yv[i] + dtv * a[i] / 2.0;
-        rhs(pot, ynk, a);
+        rhs(pot, tn + dtv / 2.0, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) yn1[i] += dtv * a[i] / 3.0;
 #pragma unroll
         for (int i = 0; i < 6; i++) ynk[i] = yv[i] + dtv * a[i] / 2.0;
-        rhs(pot, ynk, a);
+        rhs(pot, tn + dtv / 2.0, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) yn1[i] += dtv * a[i] / 3.0;
 #pragma unroll
         for (int i = 0; i < 6; i++) ynk[i] = yv[i] + dtv * a[i];
-        rhs(pot, ynk, a);
+        rhs(pot, tn + dtv, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) yn1[i] += dtv * a[i] / 6.0;
     }
 
     // rk4_estimate_step (dopr54.rs:210-368).
-    __device__ __forceinline__ double rk4_estimate_step(const Pot &pot, double dtv,
+    __device__ __forceinline__ double rk4_estimate_step(const Pot &pot, double t0, double dtv,
                                                         const Dopr54Tol &tol) const
     {
         using namespace dopr54c;
@@ -147,11 +149,11 @@ struct Dopr54Lane {
                 y1[i] = yn[i];
                 y21[i] = yn[i];
             }
-            rk4_onestep(pot, yn, y1, dtv);
-            rk4_onestep(pot, yn, y21, dtv / 2.0);
+            rk4_onestep(pot, t0, yn, y1, dtv);
+            rk4_onestep(pot, t0, yn, y21, dtv / 2.0);
 #pragma unroll
             for (int i = 0; i < 6; i++) y2[i] = y21[i];
-            rk4_onestep(pot, y21, y2, dtv / 2.0);
+            rk4_onestep(pot, t0 + dtv / 2.0, y21, y2, dtv / 2.0);
             double q = 0.0;
 #pragma unroll
             for (int i = 0; i < 6; i++) {
@@ -181,9 +183,9 @@ struct Dopr54Lane {
         double t0 = grid.at(0);
         dt = grid.at(1) - t0;
         dt_one = dt_one_init;
-        if (dt_one == -9999.99) dt_one = rk4_estimate_step(pot, dt, tol);
+        if (dt_one == -9999.99) dt_one = rk4_estimate_step(pot, t0, dt, tol);
         to = t0;
-        rhs(pot, yn, a1);
+        rhs(pot, to, yn, a1);
         ii = 0;
         done = (grid.nt < 2);
         init_to = to;
@@ -241,13 +243,13 @@ struct Dopr54Lane {
             yerr[i] = BE1 * k1[i];
             ynk[i] = yn[i] + A21 * k1[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + C2 * h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             k2[i] = h * a[i];
             ynk[i] = yn[i] + A31 * k1[i] + A32 * k2[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + C3 * h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             k3[i] = h * a[i];
@@ -255,7 +257,7 @@ struct Dopr54Lane {
             yerr[i] += BE3 * k3[i];
             ynk[i] = yn[i] + A41 * k1[i] + A42 * k2[i] + A43 * k3[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + C4 * h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             k4[i] = h * a[i];
@@ -263,7 +265,7 @@ struct Dopr54Lane {
             yerr[i] += BE4 * k4[i];
             ynk[i] = yn[i] + A51 * k1[i] + A52 * k2[i] + A53 * k3[i] + A54 * k4[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + C5 * h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             k5[i] = h * a[i];
@@ -271,7 +273,7 @@ struct Dopr54Lane {
             yerr[i] += BE5 * k5[i];
             ynk[i] = yn[i] + A61 * k1[i] + A62 * k2[i] + A63 * k3[i] + A64 * k4[i] + A65 * k5[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) {
             k6[i] = h * a[i];
@@ -279,7 +281,7 @@ struct Dopr54Lane {
             yerr[i] += BE6 * k6[i];
             ynk[i] = yn[i] + A71 * k1[i] + A73 * k3[i] + A74 * k4[i] + A75 * k5[i] + A76 * k6[i];
         }
-        rhs(pot, ynk, a);
+        rhs(pot, to + h, ynk, a);
 #pragma unroll
         for (int i = 0; i < 6; i++) yerr[i] += BE7 * h * a[i];
 

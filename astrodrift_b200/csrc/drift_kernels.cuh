@@ -57,6 +57,25 @@ __device__ __forceinline__ int segment_of(const KernelArgs &a, int64_t p)
     return lo;
 }
 
+// The potential functor of a launch: the descriptor's potential, or the
+// summed force model held in the kernel's parameter space.
+template <class Pot>
+__device__ __forceinline__ Pot make_pot(const KernelArgs &a, const double *table)
+{
+    return Pot(a.potential, table);
+}
+template <>
+__device__ __forceinline__ Composite make_pot<Composite>(const KernelArgs &a, const double *table)
+{
+    return Composite(&a.model, table);
+}
+
+template <class Pot>
+__host__ __device__ constexpr bool needs_bulge_table()
+{
+    return std::is_same<Pot, Bovy>::value || std::is_same<Pot, Composite>::value;
+}
+
 // Launch bounds of the integration kernels: at most DRIFT_MAX_THREADS
 // threads per block, and registers allocated so that DRIFT_MIN_BLOCKS_PER_SM
 // such blocks can be resident on one SM.
@@ -72,7 +91,7 @@ __device__ __forceinline__ int segment_of(const KernelArgs &a, int64_t p)
 __host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
 {
     return (method == DRIFT_DOP853 ? 24 * sizeof(double) * block : 0) +
-           (kind == DRIFT_POT_BOVY ? sizeof(BulgeTable) : 0);
+           ((kind == DRIFT_POT_BOVY || kind == DRIFT_POT_MODEL) ? sizeof(BulgeTable) : 0);
 }
 
 // TAPE (DOP853 only): record every accepted step of every particle in
@@ -87,11 +106,11 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
     // [park tile (DOP853)][bulge table (Bovy)]
     volatile double *park = smem + threadIdx.x;
     double *table = smem + (METHOD == DRIFT_DOP853 ? 24 * blockDim.x : 0);
-    if (std::is_same<Pot, Bovy>::value) {
+    if (needs_bulge_table<Pot>()) {
         for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
         __syncthreads();
     }
-    const Pot pot(a.potential, table);
+    const Pot pot = make_pot<Pot>(a, table);
     const int64_t gtid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t deadline = a.timeout_ns ? global_timer_ns() + a.timeout_ns : 0;
 
@@ -266,14 +285,14 @@ __global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ Kerne
     __shared__ unsigned hist[ORDER_BUCKETS];
     __shared__ double table[BULGE_TABLE_SIZE];
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
-    if (std::is_same<Pot, Bovy>::value)
+    if (needs_bulge_table<Pot>())
         for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
     __syncthreads();
-    const Pot pot(a.potential, table);
+    const Pot pot = make_pot<Pot>(a, table);
     for (int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pid < a.n;
          pid += (int64_t)gridDim.x * blockDim.x) {
         const double *y;
-        double span;
+        double span, t_start;
         int64_t nt = a.nt;
         if (a.nsegs) {
             const Segment &S = a.segs[segment_of(a, pid)];
@@ -281,12 +300,14 @@ __global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ Kerne
             y = S.y0 + p * 6;
             nt = S.nt;
             span = S.ts ? fabs(__ldg(S.ts + S.nt - 1) - __ldg(S.ts)) : fabs(__ldg(S.t_end + p) - S.t0);
+            t_start = S.ts ? __ldg(S.ts) : S.t0;
         } else {
             y = a.y0 + pid * 6;
             span = a.ts ? fabs(__ldg(a.ts + a.nt - 1) - __ldg(a.ts)) : fabs(__ldg(a.t_end + pid) - a.t0);
+            t_start = a.ts ? __ldg(a.ts) : a.t0;
         }
         double ax, ay, az;
-        pot.force(y[0], y[1], y[2], ax, ay, az);
+        force_at(pot, t_start, y[0], y[1], y[2], ax, ay, az);
         double r2 = fmax(y[0] * y[0] + y[1] * y[1] + y[2] * y[2], 1e-300);
         double v2 = y[3] * y[3] + y[4] * y[4] + y[5] * y[5];
         double f = sqrt(ax * ax + ay * ay + az * az);
@@ -353,6 +374,7 @@ inline cudaError_t build_order_impl(const KernelArgs &a, int method, uint8_t *ke
     case DRIFT_POT_KEPLER_CARTESIAN:
         rank_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(a, method, keys, counts);
         break;
+    case DRIFT_POT_MODEL: rank_kernel<Composite><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
     default: return cudaErrorInvalidValue;
     }
     order_scan_kernel<<<1, ORDER_BUCKETS, 0, stream>>>(counts);
@@ -395,6 +417,54 @@ inline cudaError_t force_impl(const drift_potential &p, int64_t n, const double 
     return cudaGetLastError();
 }
 
+// Acceleration of a force model at time t (drift_force_model_eval).
+__global__ void __launch_bounds__(256) model_force_kernel(const __grid_constant__ drift_force_model m,
+                                                          const __grid_constant__ BulgeTable bt, double t,
+                                                          int64_t n, const double *xyz, double *acc)
+{
+    __shared__ double table[BULGE_TABLE_SIZE];
+    for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+    __syncthreads();
+    const Composite pot(&m, table);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double ax, ay, az;
+        pot.force_t(t, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], ax, ay, az);
+        acc[3 * i] = ax;
+        acc[3 * i + 1] = ay;
+        acc[3 * i + 2] = az;
+    }
+}
+
+// One thread per (segment k, source j): accelerations at both ends from the
+// sources' own force model, then the quintic Hermite coefficients of each
+// axis, written as origins[(k * n_sources + j) * 18 + 6 * axis + c].
+__global__ void __launch_bounds__(256) origin_table_kernel(const __grid_constant__ drift_force_model m,
+                                                           const __grid_constant__ BulgeTable bt,
+                                                           int64_t n_sources, int64_t nt, double t0,
+                                                           double dt, const double *traj, double *origins)
+{
+    __shared__ double table[BULGE_TABLE_SIZE];
+    for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+    __syncthreads();
+    const Composite pot(&m, table);
+    const int64_t total = (nt - 1) * n_sources;
+    for (int64_t w = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; w < total;
+         w += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = w / n_sources, j = w - k * n_sources;
+        const double *q0 = traj + (k * n_sources + j) * 6;
+        const double *q1 = traj + ((k + 1) * n_sources + j) * 6;
+        const double ta = t0 + dt * (double)k;
+        const double tb = t0 + dt * (double)(k + 1);
+        double a0[3], a1[3];
+        pot.force_t(ta, q0[0], q0[1], q0[2], a0[0], a0[1], a0[2]);
+        pot.force_t(tb, q1[0], q1[1], q1[2], a1[0], a1[1], a1[2]);
+        double *c = origins + w * 18;
+        for (int axis = 0; axis < 3; axis++)
+            hermite5(q0[axis], q0[3 + axis], a0[axis], q1[axis], q1[3 + axis], a1[axis], dt, c + 6 * axis);
+    }
+}
+
 // Host-side launcher for this precision unit.
 inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int block,
                                cudaStream_t stream)
@@ -415,6 +485,7 @@ inline cudaError_t launch_impl(const KernelArgs &a, int method, int grid, int bl
     case DRIFT_POT_PLUMMER: DRIFT_LAUNCH(M, Plummer);                            \
     case DRIFT_POT_BOVY: DRIFT_LAUNCH(M, Bovy);                                  \
     case DRIFT_POT_KEPLER_CARTESIAN: DRIFT_LAUNCH(M, KeplerCartesian);           \
+    case DRIFT_POT_MODEL: DRIFT_LAUNCH(M, Composite);                            \
     default: return cudaErrorInvalidValue;                                       \
     }
     if (method == DRIFT_DOP853) {
@@ -443,6 +514,7 @@ inline cudaError_t occupancy_impl(int method, int kind, int block, bool tape, in
     case DRIFT_POT_PLUMMER: DRIFT_OCC(M, Plummer);                              \
     case DRIFT_POT_BOVY: DRIFT_OCC(M, Bovy);                                    \
     case DRIFT_POT_KEPLER_CARTESIAN: DRIFT_OCC(M, KeplerCartesian);             \
+    case DRIFT_POT_MODEL: DRIFT_OCC(M, Composite);                              \
     default: return cudaErrorInvalidValue;                                      \
     }
     if (method == DRIFT_DOP853) {

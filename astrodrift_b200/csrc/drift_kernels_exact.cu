@@ -15,6 +15,22 @@ cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, 
 {
     return exact::force_impl(p, n, xyz, acc, bt, grid, stream);
 }
+cudaError_t model_force_exact(const drift_force_model &m, const BulgeTable &bt, double t, int64_t n,
+                              const double *xyz, double *acc, int grid, cudaStream_t stream)
+{
+    exact::model_force_kernel<<<grid, 256, 0, stream>>>(m, bt, t, n, xyz, acc);
+    return cudaGetLastError();
+}
+cudaError_t origin_table_exact(const drift_force_model &source_model, const BulgeTable &bt,
+                               int64_t n_sources, int64_t nt, double t0, double dt,
+                               const double *trajectory, double *origins, cudaStream_t stream)
+{
+    const int64_t work = (nt - 1) * n_sources;
+    const int grid = (int)std::min<int64_t>((work + 255) / 256, 4096);
+    exact::origin_table_kernel<<<grid, 256, 0, stream>>>(source_model, bt, n_sources, nt, t0, dt,
+                                                         trajectory, origins);
+    return cudaGetLastError();
+}
 int max_threads_exact() { return exact::max_threads_impl(); }
 cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
                         uint32_t *order, int sm_count, cudaStream_t stream)

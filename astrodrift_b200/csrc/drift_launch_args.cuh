@@ -6,6 +6,7 @@
 
 #include "drift_b200.h"
 #include "drift_dopr54.cuh"
+#include "drift_composite.cuh"
 #include "drift_potentials.cuh"
 
 namespace drift {
@@ -59,7 +60,8 @@ struct KernelArgs {
     int64_t tape_steps;          // tape rows per particle
     int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
     drift_potential potential;
-    BulgeTable bulge;            // Bovy only: lower incomplete gamma table
+    BulgeTable bulge;            // Bovy (or a force model with Bovy parts): incomplete gamma table
+    drift_force_model model;     // potential.kind == DRIFT_POT_MODEL: the summed force
     Segment segs[MAX_BATCH];  // batched launch: the request table (kernel parameter space)
 };
 
@@ -81,6 +83,15 @@ cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned
                         uint32_t *order, int sm_count, cudaStream_t stream);
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
                         const BulgeTable &bt, int grid, cudaStream_t stream);
+// Force model at time t (exact unit).
+cudaError_t model_force_exact(const drift_force_model &m, const BulgeTable &bt, double t, int64_t n,
+                              const double *xyz, double *acc, int grid, cudaStream_t stream);
+// Quintic Hermite origin table of n_sources sources from their trajectory
+// (nt, n_sources, 6) on the uniform grid t0 + k dt, accelerations from the
+// sources' own force model (exact unit).
+cudaError_t origin_table_exact(const drift_force_model &source_model, const BulgeTable &bt,
+                               int64_t n_sources, int64_t nt, double t0, double dt,
+                               const double *trajectory, double *origins, cudaStream_t stream);
 cudaError_t occupancy_fma(int method, int kind, int block, bool tape, int *blocks_per_sm);
 
 }  // namespace drift

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DRIFT_ABI_VERSION 2
+#define DRIFT_ABI_VERSION 3
 
 /* Sentinel that asks DOPR54 for galpy's RK4 initial-step estimate
  * (src/integrators/galpy/mod.rs:8). */
@@ -50,7 +50,10 @@ typedef enum {
      * with a power-law-with-cutoff bulge */
     DRIFT_POT_BOVY = 2,
     /* KeplerPotential::force, Cartesian (shared/src/potential.rs:217-239) */
-    DRIFT_POT_KEPLER_CARTESIAN = 3
+    DRIFT_POT_KEPLER_CARTESIAN = 3,
+    /* The sum described by drift_launch.force_model: stationary potentials
+     * plus potentials attached to moving particle groups. */
+    DRIFT_POT_MODEL = 4
 } drift_potential_kind;
 
 typedef enum {
@@ -116,6 +119,46 @@ typedef struct {
     double bulge_gamma_s;  /* complete Gamma(s) */
 } drift_potential;
 
+/* ---- force models: a stage's force from the container graph ------------
+ * A stage's particles feel the sum of every potential their container
+ * requires (src/tree/mod.rs:89-110): stationary backgrounds, and potentials
+ * attached to particle groups integrated in earlier stages, which move along
+ * those groups' trajectories (the reference's CustomKepler / CustomPlummer
+ * recipes and CustomOrigin, shared/src/model.rs:183-234,
+ * shared/src/potential.rs:264-356).  A moving source particle's position
+ * between two output times is the quintic Hermite interpolant of its
+ * position, velocity and acceleration at both ends (drift_origin_table). */
+
+/* Largest number of summed stationary potentials, and of source groups
+ * (shared/src/lib.rs:21: at most 11 model components). */
+#define DRIFT_MAX_COMPONENTS 11
+
+/* A particle group whose particles each carry a point-mass (Kepler,
+ * Cartesian form) or Plummer potential. */
+typedef struct {
+    int32_t kind;          /* DRIFT_POT_KEPLER_CARTESIAN or DRIFT_POT_PLUMMER */
+    int32_t reserved;
+    double amp;            /* mass of each source particle */
+    double b;              /* Plummer radius */
+    int64_t first;         /* this group's sources are origins [first, first + count) */
+    int64_t count;
+} drift_source_group;
+
+typedef struct {
+    int32_t n_static;      /* stationary potentials, summed in order */
+    int32_t n_groups;      /* moving source groups, summed after them in order */
+    drift_potential statics[DRIFT_MAX_COMPONENTS];   /* kinds 0..3; Bovy parts share alpha */
+    drift_source_group groups[DRIFT_MAX_COMPONENTS];
+    int64_t n_sources;     /* all source particles */
+    int64_t n_segments;    /* origin table: segment k covers [t0 + k dt, t0 + (k+1) dt] */
+    double t0, dt;
+    const double *origins; /* (n_segments, n_sources, 18): per axis the 6 coefficients of
+                            * x(s) = c0 + s (c1 + s (c2 + s (c3 + s (c4 + s c5)))),
+                            * s = (t - t0)/dt - k; device pointer for device entry points,
+                            * host pointer for drift_integrate_host.  Times outside
+                            * [t0, t0 + n_segments dt] use the nearest segment. */
+} drift_force_model;
+
 /* One integration request.  Pointers are DEVICE pointers for drift_integrate
  * and HOST pointers for drift_integrate_host. */
 typedef struct {
@@ -149,6 +192,9 @@ typedef struct {
      * batched launches. */
     double *tape;
     int64_t tape_steps;
+    /* With potential.kind == DRIFT_POT_MODEL: the summed force (see
+     * drift_force_model); otherwise ignored. */
+    const drift_force_model *force_model;
 } drift_launch;
 
 /* Library / device information. */
@@ -206,6 +252,22 @@ int drift_integrate_batch(const drift_launch *requests, int32_t count, void *str
  * through its Potential trait (shared/src/potential.rs:41-44). */
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream);
+
+/* Origin table of moving sources (no counterpart in the reference, whose
+ * CustomOrigin tables are never built: shared/src/model.rs:193-199).
+ * trajectory (nt, n_sources, 6): the sources' states at the uniform times
+ * t0 + k dt, k = 0..nt-1, as their own stage produced them; source_model:
+ * the force that stage integrated in (its accelerations at the samples
+ * complete the Hermite data).  Writes origins (nt - 1, n_sources, 18).
+ * Device pointers. */
+int drift_origin_table(const drift_force_model *source_model, int64_t n_sources, int64_t nt,
+                       double t0, double dt, const double *trajectory, double *origins,
+                       void *stream);
+
+/* Acceleration of a force model at time t: xyz (n, 3) -> acc (n, 3), device
+ * pointers, rounded without multiply-add contraction like drift_force. */
+int drift_force_model_eval(const drift_force_model *model, int64_t n, double t,
+                           const double *xyz, double *acc, void *stream);
 
 /* ---- discrete adjoint (no counterpart in the reference) ----------------- */
 

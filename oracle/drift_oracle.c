@@ -211,13 +211,102 @@ void oracle_force(const oracle_potential *p, double x, double y, double z, doubl
     }
 }
 
-/* kepler_rhs, dopr54.rs:59-73: a = (v, F(x)). */
+/* ------------------------------------------------------------------ */
+/* Force models: stationary parts plus moving sources                  */
+/* ------------------------------------------------------------------ */
+
+static void hermite5(double x0, double v0, double a0, double x1, double v1, double a1, double h,
+                     double *c)
+{
+    const double hh = h * h;
+    const double d = x1 - x0;
+    c[0] = x0;
+    c[1] = h * v0;
+    c[2] = 0.5 * (hh * a0);
+    c[3] = 10.0 * d - h * (6.0 * v0 + 4.0 * v1) - hh * (1.5 * a0 - 0.5 * a1);
+    c[4] = -15.0 * d + h * (8.0 * v0 + 7.0 * v1) + hh * (1.5 * a0 - a1);
+    c[5] = 6.0 * d - 3.0 * h * (v0 + v1) - hh * (0.5 * a0 - 0.5 * a1);
+}
+
+static double quintic(const double *c, double s)
+{
+    return c[0] + s * (c[1] + s * (c[2] + s * (c[3] + s * (c[4] + s * c[5]))));
+}
+
+static void model_force(const oracle_model *m, double t, double x, double y, double z, double *ax,
+                        double *ay, double *az)
+{
+    double sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int i = 0; i < m->n_static; i++) {
+        double fx, fy, fz;
+        oracle_force(&m->statics[i], x, y, z, &fx, &fy, &fz);
+        sx = sx + fx;
+        sy = sy + fy;
+        sz = sz + fz;
+    }
+    if (m->n_groups > 0) {
+        const double u = (t - m->t0) / m->dt;
+        double kf = floor(u);
+        kf = fmin(fmax(kf, 0.0), (double)(m->n_segments - 1));
+        const double s = u - kf;
+        const double *row = m->origins + (int64_t)kf * m->n_sources * 18;
+        for (int g = 0; g < m->n_groups; g++) {
+            const oracle_source_group *G = &m->groups[g];
+            for (int64_t j = G->first; j < G->first + G->count; j++) {
+                const double *c = row + j * 18;
+                const double dx = x - quintic(c, s);
+                const double dy = y - quintic(c + 6, s);
+                const double dz = z - quintic(c + 12, s);
+                double fx, fy, fz;
+                if (G->kind == ORACLE_POT_PLUMMER)
+                    plummer(G->amp, G->b, dx, dy, dz, &fx, &fy, &fz);
+                else
+                    kepler_cartesian(G->amp, dx, dy, dz, &fx, &fy, &fz);
+                sx = sx + fx;
+                sy = sy + fy;
+                sz = sz + fz;
+            }
+        }
+    }
+    *ax = sx;
+    *ay = sy;
+    *az = sz;
+}
+
+void oracle_force_t(const oracle_potential *p, double t, double x, double y, double z, double *ax,
+                    double *ay, double *az)
+{
+    if (p->kind == ORACLE_POT_MODEL)
+        model_force(p->model, t, x, y, z, ax, ay, az);
+    else
+        oracle_force(p, x, y, z, ax, ay, az);
+}
+
+void oracle_origin_table(const oracle_potential *source_pot, int64_t n_sources, int64_t nt, double t0,
+                         double dt, const double *trajectory, double *origins)
+{
+    for (int64_t k = 0; k + 1 < nt; k++)
+        for (int64_t j = 0; j < n_sources; j++) {
+            const double *q0 = trajectory + (k * n_sources + j) * 6;
+            const double *q1 = trajectory + ((k + 1) * n_sources + j) * 6;
+            const double ta = t0 + dt * (double)k;
+            const double tb = t0 + dt * (double)(k + 1);
+            double a0[3], a1[3];
+            oracle_force_t(source_pot, ta, q0[0], q0[1], q0[2], &a0[0], &a0[1], &a0[2]);
+            oracle_force_t(source_pot, tb, q1[0], q1[1], q1[2], &a1[0], &a1[1], &a1[2]);
+            double *c = origins + (k * n_sources + j) * 18;
+            for (int axis = 0; axis < 3; axis++)
+                hermite5(q0[axis], q0[3 + axis], a0[axis], q1[axis], q1[3 + axis], a1[axis], dt,
+                         c + 6 * axis);
+        }
+}
+
+/* kepler_rhs, dopr54.rs:59-73: a = (v, F(t, x)). */
 static void rhs(const oracle_potential *p, double t, const double *q, double *a,
                 oracle_stats *st)
 {
-    (void)t;
     double ax, ay, az;
-    oracle_force(p, q[0], q[1], q[2], &ax, &ay, &az);
+    oracle_force_t(p, t, q[0], q[1], q[2], &ax, &ay, &az);
     a[0] = q[3];
     a[1] = q[4];
     a[2] = q[5];

@@ -34,7 +34,8 @@ enum {
     ORACLE_POT_KEPLER = 0,
     ORACLE_POT_PLUMMER = 1,
     ORACLE_POT_BOVY = 2,
-    ORACLE_POT_KEPLER_CARTESIAN = 3
+    ORACLE_POT_KEPLER_CARTESIAN = 3,
+    ORACLE_POT_MODEL = 4    /* the sum described by oracle_potential.model */
 };
 
 enum { ORACLE_DOPR54 = 0, ORACLE_DOP853 = 1 };
@@ -55,7 +56,38 @@ typedef struct {
     double bulge_rc;     /* cutoff radius                               */
     double bulge_k;      /* F_r = -bulge_k * gamma(s, r^2/rc^2) / r^2   */
     double bulge_gamma_s;/* complete Gamma(s), s = 1.5 - alpha/2        */
+    const struct oracle_model *model; /* ORACLE_POT_MODEL only                */
 } oracle_potential;
+
+/* A stage's summed force: stationary potentials, then potentials attached to
+ * moving source particles (Kepler, Cartesian form, or Plummer), each placed at
+ * its quintic Hermite origin (see oracle_origin_table).  Mirrors the device's
+ * drift_force_model and its evaluation order. */
+typedef struct {
+    int32_t kind;         /* ORACLE_POT_KEPLER_CARTESIAN or ORACLE_POT_PLUMMER */
+    int32_t pad_;
+    double amp, b;
+    int64_t first, count;
+} oracle_source_group;
+
+typedef struct oracle_model {
+    int32_t n_static, n_groups;
+    oracle_potential statics[11];
+    oracle_source_group groups[11];
+    int64_t n_sources, n_segments;
+    double t0, dt;
+    const double *origins;  /* (n_segments, n_sources, 18) */
+} oracle_model;
+
+/* Force at time t (stationary kinds ignore t). */
+void oracle_force_t(const oracle_potential *p, double t, double x, double y, double z,
+                    double *ax, double *ay, double *az);
+
+/* Quintic Hermite origin table of n_sources sources from their trajectory
+ * (nt, n_sources, 6) at the times t0 + k dt; accelerations from `source_pot`
+ * (the force the sources were integrated in).  Writes (nt-1, n_sources, 18). */
+void oracle_origin_table(const oracle_potential *source_pot, int64_t n_sources, int64_t nt, double t0,
+                         double dt, const double *trajectory, double *origins);
 
 typedef struct {
     int64_t accepted;    /* steps that advanced the solution            */

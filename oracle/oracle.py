@@ -50,6 +50,29 @@ class Potential(ctypes.Structure):
         ("bulge_rc", ctypes.c_double),
         ("bulge_k", ctypes.c_double),
         ("bulge_gamma_s", ctypes.c_double),
+        ("model", ctypes.c_void_p),
+    ]
+
+
+POT_KEPLER_CARTESIAN, POT_MODEL = 3, 4
+
+
+class SourceGroup(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int32), ("pad_", ctypes.c_int32), ("amp", ctypes.c_double),
+                ("b", ctypes.c_double), ("first", ctypes.c_int64), ("count", ctypes.c_int64)]
+
+
+class Model(ctypes.Structure):
+    _fields_ = [
+        ("n_static", ctypes.c_int32),
+        ("n_groups", ctypes.c_int32),
+        ("statics", Potential * 11),
+        ("groups", SourceGroup * 11),
+        ("n_sources", ctypes.c_int64),
+        ("n_segments", ctypes.c_int64),
+        ("t0", ctypes.c_double),
+        ("dt", ctypes.c_double),
+        ("origins", ctypes.c_void_p),
     ]
 
 
@@ -104,6 +127,9 @@ def lib() -> ctypes.CDLL:
             ctypes.c_int64, dp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
         ]
+        _lib.oracle_force_t.argtypes = [ctypes.POINTER(Potential)] + [ctypes.c_double] * 4 + [dp] * 3
+        _lib.oracle_origin_table.argtypes = [ctypes.POINTER(Potential), ctypes.c_int64, ctypes.c_int64,
+                                             ctypes.c_double, ctypes.c_double, dp, dp]
         _lib.oracle_grid_sample.restype = ctypes.c_double
         _lib.oracle_grid_sample.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int64, ctypes.c_int64]
     return _lib
@@ -127,6 +153,48 @@ def bovy(mn_amp: float = BOVY_MN_AMP, mn_a: float = BOVY_MN_A, mn_b: float = BOV
 
 def _dptr(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def model(statics=(), groups=(), *, origins=None, t0=0.0, dt=1.0, n_sources=0) -> Potential:
+    """A summed force: `statics` (Potentials) then `groups`, each
+    (kind, amp, b, first, count) with kind POT_KEPLER_CARTESIAN or POT_PLUMMER,
+    placed by `origins` (n_segments, n_sources, 18).  The returned Potential
+    keeps the model and table alive."""
+    m = Model()
+    m.n_static = len(statics)
+    for i, p in enumerate(statics):
+        m.statics[i] = p
+    m.n_groups = len(groups)
+    for i, (kind, amp, b, first, count) in enumerate(groups):
+        m.groups[i] = SourceGroup(kind=kind, amp=amp, b=b, first=first, count=count)
+    keep = None
+    if origins is not None:
+        keep = np.ascontiguousarray(origins, dtype=np.float64)
+        m.origins = keep.ctypes.data
+        m.n_segments = keep.shape[0]
+        m.n_sources = keep.shape[1]
+    else:
+        m.n_sources = n_sources
+    m.t0, m.dt = t0, dt
+    pot = Potential(kind=POT_MODEL)
+    pot.model = ctypes.addressof(m)
+    pot._keep = (m, keep)
+    return pot
+
+
+def origin_table(source_pot: Potential, trajectory: np.ndarray, t0: float, dt: float) -> np.ndarray:
+    """Quintic Hermite origin table (nt-1, n_sources, 18) of a source trajectory (nt, n_sources, 6)."""
+    traj = np.ascontiguousarray(trajectory, dtype=np.float64)
+    nt, ns = traj.shape[0], traj.shape[1]
+    out = np.zeros((nt - 1, ns, 18))
+    lib().oracle_origin_table(ctypes.byref(source_pot), ns, nt, t0, dt, _dptr(traj), _dptr(out))
+    return out
+
+
+def force_t(pot: Potential, t: float, x: float, y: float, z: float) -> tuple[float, float, float]:
+    out = (ctypes.c_double(), ctypes.c_double(), ctypes.c_double())
+    lib().oracle_force_t(ctypes.byref(pot), t, x, y, z, *(ctypes.byref(o) for o in out))
+    return tuple(o.value for o in out)  # type: ignore[return-value]
 
 
 def force(pot: Potential, x: float, y: float, z: float) -> tuple[float, float, float]:

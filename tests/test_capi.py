@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_messages():
     lib = capi.lib()
-    assert lib.drift_abi_version() == 2
+    assert lib.drift_abi_version() == 3
     assert lib.drift_result_string(0) == b"success"
     assert lib.drift_result_string(1) == b"invalid argument"
 
@@ -43,7 +43,8 @@ def test_struct_layout_matches_header(tmp_path):
 
     lines = []
     structs = (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch),
-               ("drift_adjoint_launch", capi.DriftAdjointLaunch))
+               ("drift_adjoint_launch", capi.DriftAdjointLaunch), ("drift_source_group", capi.DriftSourceGroup),
+               ("drift_force_model", capi.DriftForceModel))
     for struct_name, cls in structs:
         lines.append(f'printf("{struct_name} %zu\\n", sizeof({struct_name}));')
         for field, _ in cls._fields_:
@@ -140,3 +141,42 @@ def test_invalid_adjoint_launches_are_rejected(mutate, message):
     mutate(A)
     assert capi.lib().drift_integrate_adjoint(ctypes.byref(A), None) == 1
     assert message in capi.lib().drift_last_error().decode()
+
+
+def _model_launch(model):
+    y0 = np.zeros((4, 6))
+    ts = np.linspace(0.0, 1.0, 3)
+    L = capi.make_launch(capi.DOP853, capi.model_potential(), 4, 3, rtol=1e-10, atol=1e-10)
+    L.y0, L.ts = y0.ctypes.data, ts.ctypes.data
+    if model is not None:
+        L.force_model = ctypes.pointer(model)
+    return L, (y0, ts, model)
+
+
+@pytest.mark.parametrize(
+    "make, message",
+    [
+        (lambda: None, "needs force_model"),
+        (lambda: capi.force_model([capi.plummer()] * 3, [(capi.POT_BOVY, 1.0, 0.0, 0, 1)], origins=8,
+                                  n_sources=1, n_segments=1), "only Kepler and Plummer"),
+        (lambda: capi.force_model([], [(capi.POT_PLUMMER, 1.0, 0.1, 0, 2)], origins=8, n_sources=1,
+                                  n_segments=1), "exceed n_sources"),
+        (lambda: capi.force_model([], [(capi.POT_PLUMMER, 1.0, 0.1, 0, 1)], origins=None, n_sources=1,
+                                  n_segments=1), "origin table"),
+        (lambda: capi.force_model([], [(capi.POT_PLUMMER, 1.0, 0.1, 0, 1)], origins=8, n_sources=1,
+                                  n_segments=1, dt=0.0), "nonzero dt"),
+        (lambda: capi.force_model([capi.bovy(), capi.bovy(alpha=1.5)]), "share bulge_alpha"),
+    ],
+)
+def test_invalid_force_models_are_rejected_before_any_device_work(make, message):
+    L, keep = _model_launch(make())
+    assert capi.lib().drift_integrate(ctypes.byref(L), None) == 1
+    assert message in capi.lib().drift_last_error().decode()
+
+
+def test_force_model_with_too_many_parts_is_rejected():
+    m = capi.force_model([capi.plummer()] * 5)
+    m.n_static = 12
+    L, keep = _model_launch(m)
+    assert capi.lib().drift_integrate(ctypes.byref(L), None) == 1
+    assert "at most 11" in capi.lib().drift_last_error().decode()

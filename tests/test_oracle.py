@@ -185,3 +185,37 @@ def test_grid_sample_matches_output_grid(oracle):
     # shared/src/config.rs:69-85
     assert [oracle.grid_sample(0.0, 1.0, 3, i) for i in range(3)] == [0.0, 0.5, 1.0]
     assert [oracle.grid_sample(1.0, -1.0, 3, i) for i in range(3)] == [1.0, 0.0, -1.0]
+
+
+def test_origin_table_matches_samples_and_forces(oracle):
+    """Each quintic segment passes through its end samples with their
+    velocities and the source force's accelerations."""
+    sat = np.array([[1.2, 0.0, 0.05, 0.0, 1.0, 0.02]])
+    ts = np.linspace(0.0, 4.0, 9)
+    traj = oracle.integrate_batch(1, oracle.bovy(), sat, ts=ts, rtol=1e-12, atol=1e-12)["out"]
+    dt = ts[1] - ts[0]
+    table = oracle.origin_table(oracle.bovy(), traj, ts[0], dt)
+    assert table.shape == (8, 1, 18)
+    for k in range(8):
+        for axis in range(3):
+            c = table[k, 0, 6 * axis: 6 * axis + 6]
+            x0, v0 = traj[k, 0, axis], traj[k, 0, 3 + axis]
+            x1, v1 = traj[k + 1, 0, axis], traj[k + 1, 0, 3 + axis]
+            a0 = oracle.force(oracle.bovy(), *traj[k, 0, :3])[axis]
+            a1 = oracle.force(oracle.bovy(), *traj[k + 1, 0, :3])[axis]
+            assert c[0] == x0
+            assert abs(c[1] / dt - v0) < 1e-15 * max(1, abs(v0))
+            assert abs(2 * c[2] / dt ** 2 - a0) < 1e-14 * max(1, abs(a0))
+            assert abs(c.sum() - x1) < 1e-14
+            assert abs((c[1] + 2 * c[2] + 3 * c[3] + 4 * c[4] + 5 * c[5]) / dt - v1) < 1e-13
+            assert abs((2 * c[2] + 6 * c[3] + 12 * c[4] + 20 * c[5]) / dt ** 2 - a1) < 1e-11
+
+
+def test_single_part_model_is_the_potential(oracle):
+    y0 = np.array([[1.0, 0.1, 0.05, 0.0, 0.9, 0.02]])
+    ts = np.linspace(0.0, 5.0, 11)
+    for pot in (oracle.plummer(1.0, 1.0), oracle.bovy(), oracle.kepler(1.0)):
+        for method in (0, 1):
+            a = oracle.integrate_batch(method, pot, y0, ts=ts, rtol=1e-10, atol=1e-10)["out"]
+            b = oracle.integrate_batch(method, oracle.model([pot]), y0, ts=ts, rtol=1e-10, atol=1e-10)["out"]
+            np.testing.assert_array_equal(a, b)
