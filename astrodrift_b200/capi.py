@@ -49,6 +49,7 @@ EXPORTED = (
     "drift_server_destroy",
     "drift_integrate_adjoint",
     "drift_origin_table",
+    "drift_origin_table_host",
     "drift_force_model_eval",
 )
 
@@ -178,6 +179,9 @@ def lib() -> ctypes.CDLL:
         L.drift_origin_table.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_int64,
                                          ctypes.c_double, ctypes.c_double, ctypes.c_void_p, ctypes.c_void_p,
                                          ctypes.c_void_p]
+        L.drift_origin_table_host.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_int64,
+                                              ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                              ctypes.c_void_p]
         L.drift_force_model_eval.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L

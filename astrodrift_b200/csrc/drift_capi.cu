@@ -100,6 +100,7 @@ struct DeviceContext {
     cudaStream_t streams[2] = {nullptr, nullptr};
     cudaEvent_t done[2] = {nullptr, nullptr};
     DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor, origins;
+    DevBuf src_traj, src_table, src_origins;  // drift_origin_table_host
     HostBuf stage[2];
 };
 
@@ -683,6 +684,41 @@ int drift_origin_table(const drift_force_model *source_model, int64_t n_sources,
     DRIFT_CUDA_TRY(drift::origin_table_exact(*source_model, table, n_sources, nt, t0, dt, trajectory, origins,
                                              static_cast<cudaStream_t>(stream)),
                    "origin table kernel launch");
+    return DRIFT_SUCCESS;
+}
+
+int drift_origin_table_host(const drift_force_model *source_model, int64_t n_sources, int64_t nt, double t0,
+                            double dt, const double *trajectory, double *origins)
+{
+    if (!trajectory || !origins || n_sources < 1 || nt < 2)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "drift_origin_table_host: NULL pointer, n_sources < 1 or nt < 2");
+    int rc = validate_model(source_model);
+    if (rc) return rc;
+    DeviceContext *ctx = nullptr;
+    rc = current_context(&ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    cudaStream_t s = ctx->streams[0];
+    drift_force_model m = *source_model;
+    if (m.n_groups > 0) {
+        const size_t b = (size_t)m.n_segments * m.n_sources * 18 * sizeof(double);
+        DRIFT_CUDA_TRY(ctx->src_origins.ensure(b), "cudaMalloc(source origins)");
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->src_origins.ptr, m.origins, b, cudaMemcpyHostToDevice, s),
+                       "H2D source origins");
+        m.origins = ctx->src_origins.as<double>();
+    }
+    const size_t tb = (size_t)nt * n_sources * 6 * sizeof(double);
+    const size_t ob = (size_t)(nt - 1) * n_sources * 18 * sizeof(double);
+    DRIFT_CUDA_TRY(ctx->src_traj.ensure(tb), "cudaMalloc(source trajectory)");
+    DRIFT_CUDA_TRY(ctx->src_table.ensure(ob), "cudaMalloc(origin table)");
+    DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->src_traj.ptr, trajectory, tb, cudaMemcpyHostToDevice, s),
+                   "H2D source trajectory");
+    rc = drift_origin_table(&m, n_sources, nt, t0, dt, ctx->src_traj.as<double>(), ctx->src_table.as<double>(),
+                            s);
+    if (rc) return rc;
+    DRIFT_CUDA_TRY(cudaMemcpyAsync(origins, ctx->src_table.ptr, ob, cudaMemcpyDeviceToHost, s), "D2H origin table");
+    DRIFT_CUDA_TRY(cudaStreamSynchronize(s), "cudaStreamSynchronize");
     return DRIFT_SUCCESS;
 }
 

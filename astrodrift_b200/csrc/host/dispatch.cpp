@@ -4,10 +4,12 @@
 // (src/dispatch/gpu.rs:157-229, src/dispatch/mod.rs:14-34): log the request,
 // integrate each state-bearing stage in dependency order, return time-major
 // (nt, N, 6) trajectories.  Differences from the reference, by design:
-//  * the stage force comes from the model: the stationary background
-//    potential the stage requires (the reference ignores the model and always
-//    integrates a unit Kepler mass, src/dispatch/gpu.rs:155-156); potentials
-//    attached to moving particle groups are not yet force sources;
+//  * the stage force comes from the model (the reference ignores the model
+//    and always integrates a unit Kepler mass, src/dispatch/gpu.rs:155-156):
+//    the sum of every stationary background the stage requires and, with
+//    Config(attached_potentials=True), of the potentials attached to the
+//    particle groups it requires, which move along those groups'
+//    trajectories from their own, earlier stages;
 //  * per-particle failures (galpy's DOPR54 error code, step cap, timeout)
 //    raise IntegrationError, as the reference's CPU path does for DOPR54
 //    (src/dispatch/cpu.rs:35-38, src/dispatch/mod.rs:74-75);
@@ -97,6 +99,38 @@ const char *status_name(int s)
     }
 }
 
+// The force a stage integrates in: one stationary potential (the direct
+// path), or a drift_force_model with its origin table on the host.
+struct StageForce {
+    bool single = false;
+    drift_potential pot{};
+    drift_force_model model{};
+    std::vector<double> origins;  // (n_segments, n_sources, 18)
+    // The force as a model (for the accelerations of this stage's particles
+    // when a later stage uses them as moving sources).
+    drift_force_model as_model() const
+    {
+        if (!single) {
+            drift_force_model m = model;
+            m.origins = origins.empty() ? nullptr : origins.data();
+            return m;
+        }
+        drift_force_model m{};
+        m.n_static = 1;
+        m.statics[0] = pot;
+        return m;
+    }
+};
+
+drift_source_group source_group_of(const Recipe &r)
+{
+    drift_source_group g{};
+    g.kind = r.name == PotentialName::CustomPlummer ? DRIFT_POT_PLUMMER : DRIFT_POT_KEPLER_CARTESIAN;
+    g.amp = r.amp;
+    g.b = r.radius;
+    return g;
+}
+
 }  // namespace
 
 [[noreturn]] void raise_not_implemented(const std::string &msg)
@@ -139,20 +173,37 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
     const double rtol_ln = std::log(config.tolerance.rtol);
     const double atol_ln = std::log(config.tolerance.atol);
 
-    // Every stage's force source is checked before any device work starts.
-    std::vector<const Recipe *> stage_force;
+    // Every stage's force sources are checked before any device work starts;
+    // the origin tables of moving sources are built once their stage ran.
+    std::vector<StageForce> forces(plan.stages.size());
+    std::vector<std::vector<size_t>> moving(plan.stages.size());  // recipe indices
     for (size_t k = 0; k < plan.stages.size(); k++) {
         const Stage &stage = plan.stages[k];
-        std::vector<const Recipe *> backgrounds;
-        for (size_t i = 0; i < stage.recipes.size(); i++)
-            if (stage.recipe_is_background[i]) backgrounds.push_back(&stage.recipes[i]);
-        if (backgrounds.size() != 1)
+        StageForce &f = forces[k];
+        int n_static = 0;
+        for (size_t i = 0; i < stage.recipes.size(); i++) {
+            if (stage.recipe_is_background[i]) {
+                f.model.statics[n_static++] = potential_of(stage.recipes[i]);
+            } else if (config.attached_potentials) {
+                if (stage.container->t_end || stage.sources[i]->t_end)
+                    raise_not_implemented(fmt(
+                        "stage %zu: potentials attached to particle groups need the shared output grid "
+                        "(no per-particle end times)", k + 1));
+                moving[k].push_back(i);
+            }
+        }
+        if (n_static == 0 && moving[k].empty())
             raise_not_implemented(fmt(
-                "stage %zu requires %zu stationary background potentials; the GPU path integrates "
-                "exactly one (potentials attached to particle groups are not yet force sources)",
-                k + 1, backgrounds.size()));
-        stage_force.push_back(backgrounds[0]);
+                "stage %zu has no force source: it requires no stationary background potential%s", k + 1,
+                config.attached_potentials ? ""
+                                           : " (potentials attached to particle groups act only with "
+                                             "Config(attached_potentials=True))"));
+        f.model.n_static = n_static;
+        f.single = n_static == 1 && moving[k].empty();
+        if (f.single) f.pot = f.model.statics[0];
     }
+    std::vector<const Container *> stage_container;
+    for (const Stage &st : plan.stages) stage_container.push_back(st.container);
 
     std::vector<py::array_t<double>> results;
     int64_t total_particles = 0;
@@ -164,7 +215,51 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         const int64_t n = *c.num_particles;
         total_particles += n;
         DRIFT_LOG(LOG_GPU, LOG_DEBUG, fmt("stage %d: dispatching %lld particles to the GPU", stage_no, (long long)n));
-        const Recipe *force_source = stage_force[stage_no - 1];
+        StageForce &force = forces[stage_no - 1];
+        if (!moving[stage_no - 1].empty()) {
+            // Origin tables of the moving sources, from their stages' trajectories.
+            const int64_t nseg = ts.steps - 1;
+            const double dt = (ts.end - ts.start) / (double)(ts.steps - 1);
+            int64_t n_sources = 0;
+            for (size_t i : moving[stage_no - 1]) n_sources += *stage.sources[i]->num_particles;
+            force.origins.assign((size_t)nseg * n_sources * 18, 0.0);
+            int64_t first = 0;
+            int g = 0;
+            for (size_t i : moving[stage_no - 1]) {
+                const Container *src = stage.sources[i];
+                size_t si = 0;
+                while (si < stage_container.size() && stage_container[si] != src) si++;
+                const int64_t ns = *src->num_particles;
+                std::vector<double> part((size_t)nseg * ns * 18);
+                const drift_force_model src_model = forces[si].as_model();
+                const double *traj = results[si].data();
+                int rc;
+                {
+                    py::gil_scoped_release nogil;
+                    rc = drift_origin_table_host(&src_model, ns, ts.steps, ts.start, dt, traj, part.data());
+                }
+                if (rc != DRIFT_SUCCESS)
+                    throw IntegrationErrorCpp(fmt("origin table of stage %zu failed: %s (%s)", si + 1,
+                                                  drift_result_string(rc), drift_last_error()));
+                for (int64_t seg = 0; seg < nseg; seg++)
+                    std::memcpy(force.origins.data() + ((size_t)seg * n_sources + first) * 18,
+                                part.data() + (size_t)seg * ns * 18, sizeof(double) * 18 * ns);
+                drift_source_group grp = source_group_of(stage.recipes[i]);
+                grp.first = first;
+                grp.count = ns;
+                force.model.groups[g++] = grp;
+                first += ns;
+            }
+            force.model.n_groups = g;
+            force.model.n_sources = n_sources;
+            force.model.n_segments = nseg;
+            force.model.t0 = ts.start;
+            force.model.dt = dt;
+            force.model.origins = force.origins.data();
+            DRIFT_LOG(LOG_GPU, LOG_DEBUG,
+                      fmt("stage %d: force = %d stationary potential(s) + %d moving group(s) of %lld source particle(s)",
+                          stage_no, force.model.n_static, g, (long long)n_sources));
+        }
 
         drift_launch L;
         std::memset(&L, 0, sizeof(L));
@@ -174,7 +269,12 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
                      : config.schedule == Schedule::PERSISTENT ? DRIFT_SCHEDULE_PERSISTENT
                                                                : DRIFT_SCHEDULE_ORDERED;
         L.block_size = config.block_size;
-        L.potential = potential_of(*force_source);
+        if (force.single) {
+            L.potential = force.pot;
+        } else {
+            L.potential.kind = DRIFT_POT_MODEL;
+            L.force_model = &force.model;
+        }
         L.n = n;
         L.y0 = c.state->data();
         L.nt = ts.steps;

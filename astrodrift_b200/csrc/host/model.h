@@ -66,6 +66,10 @@ struct Config {
     int block_size = 0;
     int64_t max_steps = 0;
     double timeout_s = 0.0;
+    // Potentials attached to required particle groups act as moving force
+    // sources.  Off by default: the reference does not build them yet
+    // (shared/src/model.rs:193-199) and its tests expect them to exert no force.
+    bool attached_potentials = false;
 };
 
 enum class PotentialName { Kepler, Plummer, Bovy, CustomKepler, CustomPlummer };
@@ -98,6 +102,7 @@ struct Stage {
     const Container *container = nullptr;
     std::vector<Recipe> recipes;
     std::vector<bool> recipe_is_background;
+    std::vector<const Container *> sources;  // the container each recipe comes from
 };
 
 struct IntegrationPlan {

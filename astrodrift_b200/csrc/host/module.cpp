@@ -7,7 +7,7 @@
 // src/interface/selector.rs and src/interface/error.rs, keeping their names,
 // argument meaning, validation messages and exception types.  Additive
 // extensions: Config(precision=, schedule=, block_size=, max_steps=,
-// timeout=), run(stats=True), test_particles/particles(t_end=) and
+// timeout=, attached_potentials=), run(stats=True), test_particles/particles(t_end=) and
 // Potential.bovy(keyword parameters).
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
@@ -501,7 +501,7 @@ PYBIND11_MODULE(_drift, m)
     py::class_<ConfigObject>(m, "Config", "Configuration and registered container graph for an integration.")
         .def(py::init([](py::object engine, py::object method, py::object implementation, py::object ts,
                          py::object tolerance, py::object precision, py::object schedule, int block_size,
-                         int64_t max_steps, double timeout) {
+                         int64_t max_steps, double timeout, bool attached_potentials) {
                  ConfigObject c;
                  if (!engine.is_none()) c.inner.engine = extract_selector(engine, "Engine") == "CPU" ? Engine::CPU : Engine::GPU;
                  if (!method.is_none()) {
@@ -551,6 +551,7 @@ PYBIND11_MODULE(_drift, m)
                  c.inner.block_size = block_size;
                  c.inner.max_steps = max_steps;
                  c.inner.timeout_s = timeout;
+                 c.inner.attached_potentials = attached_potentials;
                  validate_configuration(c.inner);
                  return c;
              }),
@@ -558,7 +559,7 @@ PYBIND11_MODULE(_drift, m)
              py::arg("implementation") = py::none(), py::arg("ts") = py::none(),
              py::arg("tolerance") = py::none(), py::kw_only(), py::arg("precision") = py::none(),
              py::arg("schedule") = py::none(), py::arg("block_size") = 0, py::arg("max_steps") = 0,
-             py::arg("timeout") = 0.0)
+             py::arg("timeout") = 0.0, py::arg("attached_potentials") = false)
         .def("run", &ConfigObject::run, py::kw_only(), py::arg("stats") = false,
              "Integrate the registered model; results follow first-registration order.")
         .def("add", &ConfigObject::add, py::arg("node"),

@@ -70,6 +70,7 @@ std::optional<IntegrationPlan> AdjacencyMatrix::build(
             if (get(source, label) && src && src->recipe) {
                 stage.recipes.push_back(*src->recipe);
                 stage.recipe_is_background.push_back(!src->state);
+                stage.sources.push_back(src);
             }
         }
         plan.stages.push_back(std::move(stage));

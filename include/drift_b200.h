@@ -264,6 +264,11 @@ int drift_origin_table(const drift_force_model *source_model, int64_t n_sources,
                        double t0, double dt, const double *trajectory, double *origins,
                        void *stream);
 
+/* drift_origin_table with host pointers (trajectory, origins, and the
+ * source model's own origin table when it has moving sources); synchronous. */
+int drift_origin_table_host(const drift_force_model *source_model, int64_t n_sources, int64_t nt,
+                            double t0, double dt, const double *trajectory, double *origins);
+
 /* Acceleration of a force model at time t: xyz (n, 3) -> acc (n, 3), device
  * pointers, rounded without multiply-add contraction like drift_force. */
 int drift_force_model_eval(const drift_force_model *model, int64_t n, double t,

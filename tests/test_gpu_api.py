@@ -217,3 +217,44 @@ def test_broken_handler_does_not_abort_integration(cuda_device, restore_drift_lo
     logger.setLevel(logging.INFO)
     trajectory, _ = _log_config().run()
     assert trajectory.shape == (16, 50, 6)
+
+
+@pytest.mark.parametrize("method", SUPPORTED_METHODS)
+def test_attached_potentials_move_with_their_group(cuda_device, oracle, method) -> None:
+    """Config(attached_potentials=True): stars feel the Bovy background plus
+    the Plummer potentials carried by two satellites, placed along the
+    satellites' own trajectories (integrated in the stage before).  The
+    oracle repeats the chain: satellites, origin table, stars."""
+    sat_state = np.array([[1.2, 0.0, 0.05, 0.0, 1.0, 0.02], [0.0, -1.6, 0.0, 0.95, 0.0, 0.0]])
+    rng = np.random.default_rng(9)
+    stars_state = sat_state[0] + np.hstack([rng.normal(0, 0.05, (40, 3)), rng.normal(0, 0.05, (40, 3))])
+    gal = dft.background(dft.Potential.bovy())
+    sats = dft.particles(dft.Potential.plummer(0.02, 0.05), sat_state)
+    stars = dft.test_particles(stars_state)
+    sim = dft.Config(method=method, ts=(0.0, 8.0, 41), tolerance=1e-10, attached_potentials=True)
+    sim.add(sats, gal)
+    sim.add(stars, gal, sats)
+    sat_traj, background_result, star_traj = sim.run()
+    assert background_result is None
+
+    ts = np.array([oracle.grid_sample(0.0, 8.0, 41, k) for k in range(41)])
+    om = 0 if method == dft.Method.DOPR54 else 1
+    sat_ref = oracle.integrate_batch(om, oracle.bovy(), sat_state, ts=ts, rtol=1e-10, atol=1e-10)["out"]
+    assert np.abs(sat_traj - sat_ref).max() < 1e-9
+    table = oracle.origin_table(oracle.bovy(), sat_traj, 0.0, 8.0 / 40)
+    omodel = oracle.model([oracle.bovy()], [(oracle.POT_PLUMMER, 0.02, 0.05, 0, 2)], origins=table,
+                          t0=0.0, dt=8.0 / 40)
+    ref = oracle.integrate_batch(om, omodel, stars_state, ts=ts, rtol=1e-10, atol=1e-10)["out"]
+    scale = np.abs(ref).max(axis=2)
+    assert (np.abs(star_traj - ref).max(axis=2) / scale).max() < 1e-9
+
+    # without the flag the satellites exert no force (the reference's behaviour)
+    sim2 = dft.Config(method=method, ts=(0.0, 8.0, 41), tolerance=1e-10)
+    sats2 = dft.particles(dft.Potential.plummer(0.02, 0.05), sat_state)
+    stars2 = dft.test_particles(stars_state)
+    sim2.add(sats2, gal)
+    sim2.add(stars2, gal, sats2)
+    _, _, star_plain = sim2.run()
+    plain_ref = oracle.integrate_batch(om, oracle.bovy(), stars_state, ts=ts, rtol=1e-10, atol=1e-10)["out"]
+    assert np.abs(star_plain - plain_ref).max() < 1e-9
+    assert np.abs(star_plain[-1] - star_traj[-1]).max() > 1e-4

@@ -321,10 +321,26 @@ def test_run_without_a_device_fails_loudly() -> None:
         sim.run()
 
 
-def test_stage_force_needs_exactly_one_background() -> None:
+def test_moving_sources_need_the_shared_output_grid() -> None:
+    # A particle group with an attached potential is a moving force source;
+    # its origin table follows the shared grid, so per-particle end times are
+    # refused before any device work.
+    kp = dft.Potential.kepler(1.0)
+    gal = dft.background(kp)
+    sat = dft.particles(dft.Potential.plummer(0.1, 0.05), np.array([[1.0, 0.0, 0.0, 0.0, 1.0, 0.0]]),
+                        t_end=np.array([5.0]))
+    stars = dft.test_particles(np.tile([-1.0, 0.0, 0.0, 0.0, -1.0, 0.0], (4, 1)))
+    sim = dft.Config(ts=(0.0, 5.0, 11), attached_potentials=True)
+    sim.add(sat, gal)
+    sim.add(stars, gal, sat)
+    with pytest.raises(NotImplementedError, match="shared output grid"):
+        sim.run()
+
+
+def test_a_stage_without_force_source_is_refused() -> None:
     _, gmc, iso = _model()
     sim = dft.Config()
-    sim.add(gmc, iso)  # iso is a particle group, not a background
+    sim.add(gmc, iso)  # iso carries no potential; gmc has no background
     sim.add(iso, dft.background(dft.Potential.kepler(1.0)))
-    with pytest.raises(NotImplementedError, match="stationary background"):
+    with pytest.raises(NotImplementedError, match="no force source"):
         sim.run()
