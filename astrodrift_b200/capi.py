@@ -126,6 +126,8 @@ class DriftLaunch(ctypes.Structure):
         ("tape", ctypes.c_void_p),
         ("tape_steps", ctypes.c_int64),
         ("force_model", ctypes.POINTER(DriftForceModel)),
+        ("arbitrary_times", ctypes.c_int32),
+        ("reserved2", ctypes.c_int32),
     ]
 
 
@@ -285,7 +287,7 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
                    precision: int = EXACT, schedule: int = PERSISTENT, block_size: int = 0,
                    dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
                    timeout_s: float = 0.0, want_out: bool = True, out=None,
-                   model: DriftForceModel | None = None) -> dict:
+                   model: DriftForceModel | None = None, arbitrary_times: bool = False) -> dict:
     """drift_integrate_host: host arrays in, host arrays out.  With `model`
     (whose origin table is a host array), `pot` is ignored and the stage
     integrates in the summed force."""
@@ -303,6 +305,7 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
     if model is not None:
         L.potential = model_potential()
         L.force_model = ctypes.pointer(model)
+    L.arbitrary_times = int(arbitrary_times)
     if want_out and out is None:
         out = np.empty((nt, n, 6))
     res = dict(

@@ -272,6 +272,7 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.n_rejected = L->n_rejected;
     a.tape = L->tape;
     a.tape_steps = L->tape_steps;
+    a.arbitrary_times = L->arbitrary_times != 0;
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
@@ -369,7 +370,8 @@ int check_batch(const drift_launch *R, int32_t count)
         if (B.method != A.method || B.precision != A.precision || B.schedule != A.schedule ||
             B.block_size != A.block_size || std::memcmp(&B.potential, &A.potential, sizeof(A.potential)) ||
             B.rtol_ln != A.rtol_ln || B.atol_ln != A.atol_ln || B.dt_one != A.dt_one ||
-            B.max_steps != A.max_steps || B.timeout_s != A.timeout_s)
+            B.max_steps != A.max_steps || B.timeout_s != A.timeout_s ||
+            (B.arbitrary_times != 0) != (A.arbitrary_times != 0))
             return fail(DRIFT_ERROR_INVALID_ARGUMENT,
                         "batched requests must share method, precision, schedule, block size, "
                         "potential, tolerances, first step and limits");

@@ -85,6 +85,8 @@ struct Dopr54Lane {
     double dt;     // output interval (t[1] - t[0])
     double dt_one; // current step size
     double init_to, init_dt_one;
+    double end;    // end of the current output interval
+    bool arbitrary;  // intervals end at ts[ii + 1] (else every interval spans dt)
     int32_t ii;    // index of the interval being integrated
     int32_t err;   // galpy error code
     bool done;
@@ -173,9 +175,14 @@ struct Dopr54Lane {
 
     // dopr54.rs:670-770 set-up; writes y0 as output sample 0.
     template <class Out>
+    // arbitrary_times: interval i ends exactly at ts[i + 1] (output times
+    // need not be uniform); otherwise every interval spans ts[1] - ts[0]
+    // from where the previous one ended, as galpy's bovy_rk does.
     __device__ __forceinline__ void begin(const Pot &pot, const double *y0, const Grid &grid,
-                                          double dt_one_init, const Dopr54Tol &tol, Out &out)
+                                          double dt_one_init, const Dopr54Tol &tol, Out &out,
+                                          bool arbitrary_times = false)
     {
+        arbitrary = arbitrary_times;
 #pragma unroll
         for (int i = 0; i < 6; i++) yn[i] = y0[i];
         out.write(0, yn);
@@ -190,12 +197,13 @@ struct Dopr54Lane {
         done = (grid.nt < 2);
         init_to = to;
         init_dt_one = dt_one;
+        end = arbitrary ? grid.at(1) : init_to + dt;
         close_intervals(grid, out);
     }
 
     __device__ __forceinline__ bool inside_interval() const
     {
-        return (dt >= 0.0 && to < init_to + dt) || (dt < 0.0 && to > init_to + dt);
+        return (dt >= 0.0 && to < end) || (dt < 0.0 && to > end);
     }
 
     // End of dopr54_onestep's loop: save the state for every interval whose
@@ -211,6 +219,7 @@ struct Dopr54Lane {
             } else {
                 init_to = to;
                 init_dt_one = dt_one;
+                end = arbitrary ? grid.at(ii + 1) : init_to + dt;
             }
         }
     }
@@ -228,8 +237,8 @@ struct Dopr54Lane {
             accept = 1;
             if (err % 2 == 0) err += 1;
         }
-        if (dt >= 0.0 && dt_one > (init_to + dt - to)) dt_one = init_to + dt - to;
-        if (dt < 0.0 && dt_one < (init_to + dt - to)) dt_one = init_to + dt - to;
+        if (dt >= 0.0 && dt_one > (end - to)) dt_one = end - to;
+        if (dt < 0.0 && dt_one < (end - to)) dt_one = end - to;
 
         const double h = dt_one;
         double yn1[6], yerr[6], ynk[6], a[6];

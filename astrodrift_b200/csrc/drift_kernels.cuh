@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
         if (METHOD == DRIFT_DOP853)
             l853.begin(pot, y0, grid, a.rtol, a.atol, out);
         else
-            l54.begin(pot, y0, grid, a.dt_one, a.tol54, out);
+            l54.begin(pot, y0, grid, a.dt_one, a.tol54, out, a.arbitrary_times != 0);
         attempts = 0;
         nacc = 0;
         nrej = 0;

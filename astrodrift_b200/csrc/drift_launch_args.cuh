@@ -59,6 +59,7 @@ struct KernelArgs {
     double *tape;                // DOP853 step tape (t_old, h, y_old[6]) per accepted step, or NULL
     int64_t tape_steps;          // tape rows per particle
     int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
+    int32_t arbitrary_times;     // DOPR54: intervals end at ts[i + 1]
     drift_potential potential;
     BulgeTable bulge;            // Bovy (or a force model with Bovy parts): incomplete gamma table
     drift_force_model model;     // potential.kind == DRIFT_POT_MODEL: the summed force

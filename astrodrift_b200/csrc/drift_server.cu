@@ -105,7 +105,7 @@ bool compatible(const drift_launch &A, const drift_launch &B)
            batch_schedule(A) == batch_schedule(B) &&
            !std::memcmp(&A.potential, &B.potential, sizeof(A.potential)) && A.rtol_ln == B.rtol_ln &&
            A.atol_ln == B.atol_ln && A.dt_one == B.dt_one && A.max_steps == B.max_steps &&
-           A.timeout_s == B.timeout_s;
+           A.timeout_s == B.timeout_s && (A.arbitrary_times != 0) == (B.arbitrary_times != 0);
 }
 
 }  // namespace

@@ -168,6 +168,7 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
 
     std::vector<double> times(ts.steps);
     for (int64_t i = 0; i < ts.steps; i++) times[i] = ts.sample(i);
+    if (!config.times.empty()) times = config.times;  // arbitrary output times
 
     // LogTolerance::from_linear (src/integrators/galpy/mod.rs:19-24)
     const double rtol_ln = std::log(config.tolerance.rtol);
@@ -185,6 +186,10 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
             if (stage.recipe_is_background[i]) {
                 f.model.statics[n_static++] = potential_of(stage.recipes[i]);
             } else if (config.attached_potentials) {
+                if (!config.times.empty())
+                    raise_not_implemented(fmt(
+                        "stage %zu: potentials attached to particle groups need uniformly spaced "
+                        "output times", k + 1));
                 if (stage.container->t_end || stage.sources[i]->t_end)
                     raise_not_implemented(fmt(
                         "stage %zu: potentials attached to particle groups need the shared output grid "
@@ -290,6 +295,7 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         L.dt_one = DRIFT_INITIAL_STEP_SENTINEL;
         L.max_steps = config.max_steps;
         L.timeout_s = config.timeout_s;
+        L.arbitrary_times = config.arbitrary_times ? 1 : 0;
 
         py::array_t<double> out({(py::ssize_t)ts.steps, (py::ssize_t)n, (py::ssize_t)STATE_DIM});
         py::array_t<uint8_t> status(n);

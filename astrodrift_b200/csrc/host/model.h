@@ -70,6 +70,10 @@ struct Config {
     // sources.  Off by default: the reference does not build them yet
     // (shared/src/model.rs:193-199) and its tests expect them to exert no force.
     bool attached_potentials = false;
+    // Output times kept as given (Config(arbitrary_times=True) with a time
+    // list): need not be uniform.  Empty: the affine grid `output`.
+    bool arbitrary_times = false;
+    std::vector<double> times;
 };
 
 enum class PotentialName { Kepler, Plummer, Bovy, CustomKepler, CustomPlummer };

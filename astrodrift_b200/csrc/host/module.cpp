@@ -7,7 +7,7 @@
 // src/interface/selector.rs and src/interface/error.rs, keeping their names,
 // argument meaning, validation messages and exception types.  Additive
 // extensions: Config(precision=, schedule=, block_size=, max_steps=,
-// timeout=, attached_potentials=), run(stats=True), test_particles/particles(t_end=) and
+// timeout=, attached_potentials=, arbitrary_times=), run(stats=True), test_particles/particles(t_end=) and
 // Potential.bovy(keyword parameters).
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
@@ -63,7 +63,7 @@ OutputGrid grid_new(double start, double end, int64_t steps)
     return OutputGrid{start, end, steps};
 }
 
-OutputGrid grid_from_times(const double *t, int64_t len)
+OutputGrid grid_from_times(const double *t, int64_t len, bool uniform = true)
 {
     if (len < 2 || len > MAX_OUTPUT_TIMES)
         throw py::value_error("ts must contain between 2 and " + std::to_string(MAX_OUTPUT_TIMES) +
@@ -75,6 +75,7 @@ OutputGrid grid_from_times(const double *t, int64_t len)
     for (int64_t i = 0; i + 1 < len; i++)
         if (increasing ? t[i + 1] <= t[i] : t[i + 1] >= t[i])
             throw py::value_error("ts values must be strictly increasing or strictly decreasing");
+    if (!uniform) return g;
     double step = (g.end - g.start) / (double)(g.steps - 1);
     for (int64_t i = 0; i < len; i++) {
         double expected = g.sample(i);
@@ -89,7 +90,9 @@ OutputGrid grid_from_times(const double *t, int64_t len)
 }
 
 // PyOutputGrid::extract (src/interface/mod.rs:31-65)
-OutputGrid extract_grid(const py::handle &obj)
+// With `times` (Config(arbitrary_times=True)), explicit time lists need only
+// be finite and strictly monotone, and are kept as given.
+OutputGrid extract_grid(const py::handle &obj, std::vector<double> *times = nullptr)
 {
     if (py::isinstance<py::tuple>(obj)) {
         py::tuple tup = obj.cast<py::tuple>();
@@ -102,12 +105,17 @@ OutputGrid extract_grid(const py::handle &obj)
         if (arr.ndim() == 1 && arr.dtype().is(py::dtype::of<double>())) {
             if (!(arr.flags() & py::array::c_style))
                 throw py::value_error("NumPy time arrays must be contiguous");
-            return grid_from_times(static_cast<const double *>(arr.data()), arr.shape(0));
+            const double *t = static_cast<const double *>(arr.data());
+            OutputGrid g = grid_from_times(t, arr.shape(0), times == nullptr);
+            if (times) times->assign(t, t + arr.shape(0));
+            return g;
         }
     }
     try {
         std::vector<double> seq = obj.cast<std::vector<double>>();
-        return grid_from_times(seq.data(), (int64_t)seq.size());
+        OutputGrid g = grid_from_times(seq.data(), (int64_t)seq.size(), times == nullptr);
+        if (times) *times = seq;
+        return g;
     } catch (const py::cast_error &) {
     }
     throw py::value_error("Expected (start, end, steps) tuple or 1D numpy.linspace array");
@@ -501,7 +509,8 @@ PYBIND11_MODULE(_drift, m)
     py::class_<ConfigObject>(m, "Config", "Configuration and registered container graph for an integration.")
         .def(py::init([](py::object engine, py::object method, py::object implementation, py::object ts,
                          py::object tolerance, py::object precision, py::object schedule, int block_size,
-                         int64_t max_steps, double timeout, bool attached_potentials) {
+                         int64_t max_steps, double timeout, bool attached_potentials,
+                         bool arbitrary_times) {
                  ConfigObject c;
                  if (!engine.is_none()) c.inner.engine = extract_selector(engine, "Engine") == "CPU" ? Engine::CPU : Engine::GPU;
                  if (!method.is_none()) {
@@ -524,7 +533,9 @@ PYBIND11_MODULE(_drift, m)
                      else
                          throw py::value_error("invalid Implementation value");
                  }
-                 if (!ts.is_none()) c.inner.output = extract_grid(ts);
+                 c.inner.arbitrary_times = arbitrary_times;
+                 if (!ts.is_none())
+                     c.inner.output = extract_grid(ts, arbitrary_times ? &c.inner.times : nullptr);
                  if (!tolerance.is_none()) c.inner.tolerance = extract_tolerance(tolerance);
                  if (!precision.is_none()) {
                      std::string v = precision.cast<std::string>();
@@ -559,7 +570,8 @@ PYBIND11_MODULE(_drift, m)
              py::arg("implementation") = py::none(), py::arg("ts") = py::none(),
              py::arg("tolerance") = py::none(), py::kw_only(), py::arg("precision") = py::none(),
              py::arg("schedule") = py::none(), py::arg("block_size") = 0, py::arg("max_steps") = 0,
-             py::arg("timeout") = 0.0, py::arg("attached_potentials") = false)
+             py::arg("timeout") = 0.0, py::arg("attached_potentials") = false,
+             py::arg("arbitrary_times") = false)
         .def("run", &ConfigObject::run, py::kw_only(), py::arg("stats") = false,
              "Integrate the registered model; results follow first-registration order.")
         .def("add", &ConfigObject::add, py::arg("node"),

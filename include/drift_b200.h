@@ -195,6 +195,13 @@ typedef struct {
     /* With potential.kind == DRIFT_POT_MODEL: the summed force (see
      * drift_force_model); otherwise ignored. */
     const drift_force_model *force_model;
+    /* DOPR54 only: 0 = every output interval spans ts[1] - ts[0] from where
+     * the previous one ended (galpy's uniform-grid semantics, the reference's
+     * behaviour); 1 = interval i ends exactly at ts[i + 1], so the shared grid
+     * may hold arbitrary strictly monotone times.  DOP853's dense output
+     * handles arbitrary times either way. */
+    int32_t arbitrary_times;
+    int32_t reserved2;
 } drift_launch;
 
 /* Library / device information. */

@@ -506,9 +506,9 @@ static double dopr54_actualstep(const oracle_potential *p, double *yo, double dt
     return dt * pow(2.0, powertwo);
 }
 
-int oracle_dopr54(const oracle_potential *p, const double yo_in[6], int nt, double dt_one,
-                  const double *t, double rtol, double atol, int64_t max_steps,
-                  double *result, int *err, oracle_stats *stats)
+static int dopr54_run(const oracle_potential *p, const double yo_in[6], int nt, double dt_one,
+                      const double *t, double rtol, double atol, int64_t max_steps,
+                      double *result, int *err, oracle_stats *stats, int arbitrary_times)
 {
     double a[DIM], a1[DIM], k1[DIM], k2[DIM], k3[DIM], k4[DIM], k5[DIM], k6[DIM];
     double yo[DIM], yn[DIM], yn1[DIM], yerr[DIM], ynk[DIM];
@@ -535,7 +535,10 @@ int oracle_dopr54(const oracle_potential *p, const double yo_in[6], int nt, doub
         /* dopr54_onestep, dopr54.rs:370-460 */
         double init_dt_one = dt_one;
         double init_to = to;
-        while ((dt >= 0.0 && to < init_to + dt) || (dt < 0.0 && to > init_to + dt)) {
+        /* arbitrary_times: the interval ends at t[ii + 1]; otherwise it spans
+         * dt from where the previous one ended (bovy_rk's uniform grid). */
+        const double end = arbitrary_times ? t[ii + 1] : init_to + dt;
+        while ((dt >= 0.0 && to < end) || (dt < 0.0 && to > end)) {
             int accept = 0;
             int advanced;
             if (init_dt_one / dt_one > MAX_STEPREDUCE || dt_one != dt_one) {
@@ -543,8 +546,8 @@ int oracle_dopr54(const oracle_potential *p, const double yo_in[6], int nt, doub
                 accept = 1;
                 if (*err % 2 == 0) *err += 1;
             }
-            if (dt >= 0.0 && dt_one > (init_to + dt - to)) dt_one = init_to + dt - to;
-            if (dt < 0.0 && dt_one < (init_to + dt - to)) dt_one = init_to + dt - to;
+            if (dt >= 0.0 && dt_one > (end - to)) dt_one = end - to;
+            if (dt < 0.0 && dt_one < (end - to)) dt_one = end - to;
             if (max_steps > 0 && attempts >= max_steps) {
                 status = ORACLE_MAX_STEPS;
                 goto done;
@@ -727,6 +730,13 @@ static const double ER9 = -0.3503288487499736816886487290;
 static const double ER10 = 0.3341791187130174790297318841;
 static const double ER11 = 0.8192320648511571246570742613e-1;
 static const double ER12 = -0.2235530786388629525884427845e-1;
+
+int oracle_dopr54(const oracle_potential *p, const double yo_in[6], int nt, double dt_one,
+                  const double *t, double rtol, double atol, int64_t max_steps,
+                  double *result, int *err, oracle_stats *stats)
+{
+    return dopr54_run(p, yo_in, nt, dt_one, t, rtol, atol, max_steps, result, err, stats, 0);
+}
 
 static double c_min(double a, double b) { return a < b ? a : b; }
 static double c_max(double a, double b) { return a > b ? a : b; }
@@ -986,7 +996,8 @@ int64_t oracle_integrate_batch(int method, const oracle_potential *p, int64_t n,
                                const double *t_end, double rtol_ln, double atol_ln,
                                double dt_one, int64_t max_steps, double *out,
                                int32_t *status, int32_t *err, int64_t *accepted,
-                               int64_t *rejected, int64_t *rhs_count, int threads)
+                               int64_t *rejected, int64_t *rhs_count, int threads,
+                               int arbitrary_times)
 {
     int64_t failures = 0;
     if (threads < 1) threads = 1;
@@ -1005,8 +1016,8 @@ int64_t oracle_integrate_batch(int method, const oracle_potential *p, int64_t n,
             int e = 0;
             int s;
             if (method == ORACLE_DOPR54)
-                s = oracle_dopr54(p, y0 + pid * DIM, nt, dt_one, tp, rtol_ln, atol_ln, max_steps,
-                                  traj, &e, &st);
+                s = dopr54_run(p, y0 + pid * DIM, nt, dt_one, tp, rtol_ln, atol_ln, max_steps,
+                               traj, &e, &st, arbitrary_times);
             else
                 s = oracle_dop853(p, y0 + pid * DIM, nt, tp, rtol_ln, atol_ln, max_steps, traj,
                                   &st);

@@ -132,13 +132,16 @@ int oracle_dop853_tape(const oracle_potential *p, const double y0[6], int nt, co
  * or `t_end` (per-particle end times on the grid t0..t_end[i] with nt points,
  * sampled as shared/src/config.rs:57-66) is given.  Uses `threads` OpenMP
  * threads.  Per-particle outputs may be NULL.  Returns the number of
- * particles whose status is not ORACLE_OK. */
+ * particles whose status is not ORACLE_OK.  arbitrary_times (DOPR54): each
+ * output interval ends exactly at ts[i + 1] instead of spanning ts[1] - ts[0]
+ * from the previous end (the device's drift_launch.arbitrary_times). */
 int64_t oracle_integrate_batch(int method, const oracle_potential *p, int64_t n,
                                const double *y0, int nt, const double *ts, double t0,
                                const double *t_end, double rtol_ln, double atol_ln,
                                double dt_one, int64_t max_steps, double *out,
                                int32_t *status, int32_t *err, int64_t *accepted,
-                               int64_t *rejected, int64_t *rhs, int threads);
+                               int64_t *rejected, int64_t *rhs, int threads,
+                               int arbitrary_times);
 
 /* OutputGrid::sample (shared/src/config.rs:57-66). */
 double oracle_grid_sample(double start, double end, int64_t steps, int64_t index);

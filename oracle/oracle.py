@@ -125,7 +125,7 @@ def lib() -> ctypes.CDLL:
             ctypes.c_int, ctypes.POINTER(Potential), ctypes.c_int64, dp, ctypes.c_int, dp,
             ctypes.c_double, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double,
             ctypes.c_int64, dp, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
+            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
         ]
         _lib.oracle_force_t.argtypes = [ctypes.POINTER(Potential)] + [ctypes.c_double] * 4 + [dp] * 3
         _lib.oracle_origin_table.argtypes = [ctypes.POINTER(Potential), ctypes.c_int64, ctypes.c_int64,
@@ -244,7 +244,8 @@ def dop853_tape(pot: Potential, y0, t, rtol_ln: float, atol_ln: float, tape_step
 def integrate_batch(method: int, pot: Potential, y0: np.ndarray, *, ts=None, t0: float = 0.0,
                     t_end=None, nt: int | None = None, rtol: float = 1e-12, atol: float = 1e-12,
                     dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
-                    threads: int | None = None, want_output: bool = True) -> dict:
+                    threads: int | None = None, want_output: bool = True,
+                    arbitrary_times: bool = False) -> dict:
     """Batch integration restating src/dispatch/cpu.rs:53-89.
 
     Tolerances are linear; they are converted to natural logarithms with the
@@ -274,7 +275,7 @@ def integrate_batch(method: int, pot: Potential, y0: np.ndarray, *, ts=None, t0:
         math.log(rtol), math.log(atol), dt_one, max_steps,
         _dptr(out) if out is not None else None,
         status.ctypes.data, err.ctypes.data, acc.ctypes.data, rej.ctypes.data, rhs.ctypes.data,
-        threads)
+        threads, int(arbitrary_times))
     return dict(out=out, status=status, err=err, accepted=acc, rejected=rej, rhs=rhs,
                 failures=int(fails))
 

@@ -219,3 +219,20 @@ def test_single_part_model_is_the_potential(oracle):
             a = oracle.integrate_batch(method, pot, y0, ts=ts, rtol=1e-10, atol=1e-10)["out"]
             b = oracle.integrate_batch(method, oracle.model([pot]), y0, ts=ts, rtol=1e-10, atol=1e-10)["out"]
             np.testing.assert_array_equal(a, b)
+
+
+def test_arbitrary_output_times(oracle):
+    """DOPR54 with arbitrary_times lands every interval on the requested time:
+    on a logarithmic grid it agrees with DOP853's dense output to the
+    integration tolerance, and on a uniform grid with the galpy semantics."""
+    y0 = np.array([[1.0, 0.1, 0.05, 0.0, 0.9, 0.02], [0.7, -0.3, 0.0, 0.4, 0.8, 0.1]])
+    ts = np.concatenate([[0.0], np.logspace(-2, 1, 12)])
+    a = oracle.integrate_batch(0, oracle.plummer(1.0, 1.0), y0, ts=ts, rtol=1e-12, atol=1e-12,
+                               arbitrary_times=True)["out"]
+    b = oracle.integrate_batch(1, oracle.plummer(1.0, 1.0), y0, ts=ts, rtol=1e-12, atol=1e-12)["out"]
+    assert np.abs(a - b).max() < 1e-9
+    u = np.linspace(0.0, 10.0, 11)
+    c = oracle.integrate_batch(0, oracle.plummer(1.0, 1.0), y0, ts=u, rtol=1e-12, atol=1e-12,
+                               arbitrary_times=True)["out"]
+    d = oracle.integrate_batch(0, oracle.plummer(1.0, 1.0), y0, ts=u, rtol=1e-12, atol=1e-12)["out"]
+    assert np.abs(c - d).max() < 1e-10

@@ -344,3 +344,15 @@ def test_a_stage_without_force_source_is_refused() -> None:
     sim.add(iso, dft.background(dft.Potential.kepler(1.0)))
     with pytest.raises(NotImplementedError, match="no force source"):
         sim.run()
+
+
+def test_arbitrary_times_are_accepted_only_when_asked() -> None:
+    times = np.logspace(0.0, 1.0, 7)
+    with pytest.raises(ValueError, match="uniformly spaced"):
+        dft.Config(ts=times)
+    dft.Config(ts=times, arbitrary_times=True)
+    dft.Config(ts=[0.0, 0.1, 0.5, 2.0], arbitrary_times=True)
+    with pytest.raises(ValueError, match="strictly increasing or strictly decreasing"):
+        dft.Config(ts=[0.0, 1.0, 0.5], arbitrary_times=True)
+    with pytest.raises(ValueError, match="finite"):
+        dft.Config(ts=[0.0, float("nan"), 1.0], arbitrary_times=True)
