@@ -25,6 +25,7 @@
 #include "drift_b200.h"
 
 namespace py = pybind11;
+using namespace pybind11::literals;
 
 namespace drift_host {
 
@@ -105,16 +106,14 @@ struct StageForce {
     bool single = false;
     drift_potential pot{};
     drift_force_model model{};
-    std::vector<double> origins;  // (n_segments, n_sources, 18)
+    std::vector<double> origins;  // host table (n_segments, n_sources, 18)
+    py::object origins_dev;       // device table (run(device=True))
     // The force as a model (for the accelerations of this stage's particles
-    // when a later stage uses them as moving sources).
+    // when a later stage uses them as moving sources); model.origins points
+    // at the table of the current mode.
     drift_force_model as_model() const
     {
-        if (!single) {
-            drift_force_model m = model;
-            m.origins = origins.empty() ? nullptr : origins.data();
-            return m;
-        }
+        if (!single) return model;
         drift_force_model m{};
         m.n_static = 1;
         m.statics[0] = pot;
@@ -155,8 +154,8 @@ void log_record(const char *logger_name, int level, const char *file, int line, 
 
 #define DRIFT_LOG(logger, level, msg) log_record(logger, level, "gpu_dispatch.cpp", __LINE__, msg)
 
-std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const IntegrationPlan &plan,
-                                              std::vector<StageStats> *stats)
+std::vector<py::object> gpu_dispatch(const Config &config, const IntegrationPlan &plan,
+                                     std::vector<StageStats> *stats, bool device_out)
 {
     const OutputGrid &ts = config.output;
     DRIFT_LOG(LOG_GPU, LOG_INFO,
@@ -210,7 +209,25 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
     std::vector<const Container *> stage_container;
     for (const Stage &st : plan.stages) stage_container.push_back(st.container);
 
-    std::vector<py::array_t<double>> results;
+    std::vector<py::object> results;
+    // run(device=True): every buffer is a torch CUDA tensor on the current
+    // device and stream, trajectories stay in HBM.
+    py::object torch, dev, f64;
+    uintptr_t stream = 0;
+    if (device_out) {
+        torch = py::module_::import("torch");
+        if (!torch.attr("cuda").attr("is_available")().cast<bool>())
+            throw DriftErrorCpp("GPU integration needs a CUDA device: torch.cuda is not available");
+        dev = torch.attr("device")("cuda", torch.attr("cuda").attr("current_device")());
+        f64 = torch.attr("float64");
+        stream = torch.attr("cuda").attr("current_stream")(dev).attr("cuda_stream").cast<uintptr_t>();
+    }
+    auto to_device = [&](const double *data, py::ssize_t rows, py::ssize_t cols) {
+        py::array_t<double> host(cols ? std::vector<py::ssize_t>{rows, cols} : std::vector<py::ssize_t>{rows});
+        std::memcpy(host.mutable_data(), data, sizeof(double) * rows * (cols ? cols : 1));
+        return torch.attr("from_numpy")(host).attr("to")(dev);
+    };
+    auto ptr_of = [](const py::object &t) { return t.attr("data_ptr")().cast<uintptr_t>(); };
     int64_t total_particles = 0;
     static bool backend_announced = false;
     int stage_no = 0;
@@ -227,7 +244,11 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
             const double dt = (ts.end - ts.start) / (double)(ts.steps - 1);
             int64_t n_sources = 0;
             for (size_t i : moving[stage_no - 1]) n_sources += *stage.sources[i]->num_particles;
-            force.origins.assign((size_t)nseg * n_sources * 18, 0.0);
+            if (device_out)
+                force.origins_dev = torch.attr("empty")(py::make_tuple(nseg, n_sources, 18), "dtype"_a = f64,
+                                                        "device"_a = dev);
+            else
+                force.origins.assign((size_t)nseg * n_sources * 18, 0.0);
             int64_t first = 0;
             int g = 0;
             for (size_t i : moving[stage_no - 1]) {
@@ -235,20 +256,37 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
                 size_t si = 0;
                 while (si < stage_container.size() && stage_container[si] != src) si++;
                 const int64_t ns = *src->num_particles;
-                std::vector<double> part((size_t)nseg * ns * 18);
                 const drift_force_model src_model = forces[si].as_model();
-                const double *traj = results[si].data();
                 int rc;
-                {
-                    py::gil_scoped_release nogil;
-                    rc = drift_origin_table_host(&src_model, ns, ts.steps, ts.start, dt, traj, part.data());
+                if (device_out) {
+                    py::object part = torch.attr("empty")(py::make_tuple(nseg, ns, 18), "dtype"_a = f64,
+                                                          "device"_a = dev);
+                    const double *traj = reinterpret_cast<const double *>(ptr_of(results[si]));
+                    double *dst = reinterpret_cast<double *>(ptr_of(part));
+                    {
+                        py::gil_scoped_release nogil;
+                        rc = drift_origin_table(&src_model, ns, ts.steps, ts.start, dt, traj, dst,
+                                                reinterpret_cast<void *>(stream));
+                    }
+                    if (rc == DRIFT_SUCCESS)
+                        force.origins_dev.attr("__setitem__")(
+                            py::make_tuple(py::slice(py::none(), py::none(), py::none()),
+                                           py::slice(first, first + ns, 1)),
+                            part);
+                } else {
+                    std::vector<double> part((size_t)nseg * ns * 18);
+                    const double *traj = results[si].cast<py::array_t<double>>().data();
+                    {
+                        py::gil_scoped_release nogil;
+                        rc = drift_origin_table_host(&src_model, ns, ts.steps, ts.start, dt, traj, part.data());
+                    }
+                    for (int64_t seg = 0; rc == DRIFT_SUCCESS && seg < nseg; seg++)
+                        std::memcpy(force.origins.data() + ((size_t)seg * n_sources + first) * 18,
+                                    part.data() + (size_t)seg * ns * 18, sizeof(double) * 18 * ns);
                 }
                 if (rc != DRIFT_SUCCESS)
                     throw IntegrationErrorCpp(fmt("origin table of stage %zu failed: %s (%s)", si + 1,
                                                   drift_result_string(rc), drift_last_error()));
-                for (int64_t seg = 0; seg < nseg; seg++)
-                    std::memcpy(force.origins.data() + ((size_t)seg * n_sources + first) * 18,
-                                part.data() + (size_t)seg * ns * 18, sizeof(double) * 18 * ns);
                 drift_source_group grp = source_group_of(stage.recipes[i]);
                 grp.first = first;
                 grp.count = ns;
@@ -260,7 +298,8 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
             force.model.n_segments = nseg;
             force.model.t0 = ts.start;
             force.model.dt = dt;
-            force.model.origins = force.origins.data();
+            force.model.origins = device_out ? reinterpret_cast<const double *>(ptr_of(force.origins_dev))
+                                             : force.origins.data();
             DRIFT_LOG(LOG_GPU, LOG_DEBUG,
                       fmt("stage %d: force = %d stationary potential(s) + %d moving group(s) of %lld source particle(s)",
                           stage_no, force.model.n_static, g, (long long)n_sources));
@@ -297,15 +336,46 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         L.timeout_s = config.timeout_s;
         L.arbitrary_times = config.arbitrary_times ? 1 : 0;
 
-        py::array_t<double> out({(py::ssize_t)ts.steps, (py::ssize_t)n, (py::ssize_t)STATE_DIM});
         py::array_t<uint8_t> status(n);
         py::array_t<int32_t> err(n);
         py::array_t<uint32_t> acc(n), rej(n);
-        L.out = out.mutable_data();
-        L.status = status.mutable_data();
-        L.err_code = err.mutable_data();
-        L.n_accepted = acc.mutable_data();
-        L.n_rejected = rej.mutable_data();
+        py::object out;
+        // device mode: inputs, outputs and counters as CUDA tensors
+        py::object y0_d, grid_d, st_d, err_d, acc_d, rej_d, ws_d;
+        if (device_out) {
+            y0_d = to_device(c.state->data(), n, STATE_DIM);
+            grid_d = c.t_end ? to_device(c.t_end->data(), n, 0) : to_device(times.data(), ts.steps, 0);
+            out = torch.attr("empty")(py::make_tuple(ts.steps, n, STATE_DIM), "dtype"_a = f64, "device"_a = dev);
+            st_d = torch.attr("zeros")(n, "dtype"_a = torch.attr("uint8"), "device"_a = dev);
+            err_d = torch.attr("zeros")(n, "dtype"_a = torch.attr("int32"), "device"_a = dev);
+            acc_d = torch.attr("zeros")(n, "dtype"_a = torch.attr("int32"), "device"_a = dev);
+            rej_d = torch.attr("zeros")(n, "dtype"_a = torch.attr("int32"), "device"_a = dev);
+            L.y0 = reinterpret_cast<const double *>(ptr_of(y0_d));
+            if (c.t_end)
+                L.t_end = reinterpret_cast<const double *>(ptr_of(grid_d));
+            else
+                L.ts = reinterpret_cast<const double *>(ptr_of(grid_d));
+            L.out = reinterpret_cast<double *>(ptr_of(out));
+            L.status = reinterpret_cast<uint8_t *>(ptr_of(st_d));
+            L.err_code = reinterpret_cast<int32_t *>(ptr_of(err_d));
+            L.n_accepted = reinterpret_cast<uint32_t *>(ptr_of(acc_d));
+            L.n_rejected = reinterpret_cast<uint32_t *>(ptr_of(rej_d));
+            size_t ws_bytes = 0;
+            drift_query_workspace(&L, &ws_bytes);
+            if (ws_bytes) {
+                ws_d = torch.attr("empty")(ws_bytes, "dtype"_a = torch.attr("uint8"), "device"_a = dev);
+                L.workspace = reinterpret_cast<void *>(ptr_of(ws_d));
+                L.workspace_bytes = ws_bytes;
+            }
+        } else {
+            py::array_t<double> host_out({(py::ssize_t)ts.steps, (py::ssize_t)n, (py::ssize_t)STATE_DIM});
+            L.out = host_out.mutable_data();
+            L.status = status.mutable_data();
+            L.err_code = err.mutable_data();
+            L.n_accepted = acc.mutable_data();
+            L.n_rejected = rej.mutable_data();
+            out = host_out;
+        }
 
         const char *kernel_label = config.method == Method::DOPR54 ? "GALPY DOPR54" : "GALPY DOP853";
         DRIFT_LOG(LOG_GPU, LOG_DEBUG,
@@ -327,7 +397,18 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
         int rc;
         {
             py::gil_scoped_release nogil;
-            rc = drift_integrate_host(&L);
+            rc = device_out ? drift_integrate(&L, reinterpret_cast<void *>(stream)) : drift_integrate_host(&L);
+        }
+        if (device_out && rc == DRIFT_SUCCESS) {
+            // the small per-particle counters come back (this also waits for the stage)
+            auto fetch = [&](const py::object &t, auto &dst) {
+                py::array a = t.attr("cpu")().attr("numpy")();
+                std::memcpy(dst.mutable_data(), a.data(), a.nbytes());
+            };
+            fetch(st_d, status);
+            fetch(err_d, err);
+            fetch(acc_d, acc);
+            fetch(rej_d, rej);
         }
         const double secs =
             std::chrono::duration<double>(std::chrono::steady_clock::now() - stage_started).count();
@@ -338,7 +419,10 @@ std::vector<py::array_t<double>> gpu_dispatch(const Config &config, const Integr
                                           drift_result_string(rc), why.c_str()));
         }
         const size_t out_bytes = (size_t)ts.steps * n * STATE_DIM * sizeof(double);
-        DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, fmt("copied %zu result bytes to the host", out_bytes));
+        if (device_out)
+            DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, fmt("kept %zu result bytes on the device", out_bytes));
+        else
+            DRIFT_LOG(LOG_BACKEND, LOG_DEBUG, fmt("copied %zu result bytes to the host", out_bytes));
 
         // galpy's DOPR54 error code first (the reference's CPU error), then
         // the build's own per-particle limits.

@@ -39,9 +39,10 @@ struct StageStats {
 };
 
 // Integrates every stage of `plan`; result[i] is the (nt, N, 6) trajectory
-// of plan.stages[i].  `stats`, if non-null, receives per-stage counters.
-std::vector<pybind11::array_t<double>> gpu_dispatch(const Config &config,
-                                                    const IntegrationPlan &plan,
-                                                    std::vector<StageStats> *stats);
+// of plan.stages[i]: a numpy array, or with `device_out` a torch CUDA tensor
+// written in place by the kernels (no host round trip).  `stats`, if
+// non-null, receives per-stage counters.
+std::vector<pybind11::object> gpu_dispatch(const Config &config, const IntegrationPlan &plan,
+                                           std::vector<StageStats> *stats, bool device_out = false);
 
 }  // namespace drift_host

@@ -7,7 +7,7 @@
 // src/interface/selector.rs and src/interface/error.rs, keeping their names,
 // argument meaning, validation messages and exception types.  Additive
 // extensions: Config(precision=, schedule=, block_size=, max_steps=,
-// timeout=, attached_potentials=, arbitrary_times=), run(stats=True), test_particles/particles(t_end=) and
+// timeout=, attached_potentials=, arbitrary_times=), run(stats=True, device=True), test_particles/particles(t_end=) and
 // Potential.bovy(keyword parameters).
 #include <pybind11/numpy.h>
 #include <pybind11/pybind11.h>
@@ -313,14 +313,14 @@ struct ConfigObject {
         return *plan;
     }
 
-    py::object run(bool want_stats)
+    py::object run(bool want_stats, bool device)
     {
         validate_registered_model();
         IntegrationPlan plan = build_tree();
         validate_configuration(inner);
         std::vector<StageStats> stats;
-        std::vector<py::array_t<double>> results;
-        if (!plan.stages.empty()) results = gpu_dispatch(inner, plan, want_stats ? &stats : nullptr);
+        std::vector<py::object> results;
+        if (!plan.stages.empty()) results = gpu_dispatch(inner, plan, want_stats ? &stats : nullptr, device);
         py::list items;
         py::list stat_items;
         for (const auto &c : containers) {
@@ -572,8 +572,9 @@ PYBIND11_MODULE(_drift, m)
              py::arg("schedule") = py::none(), py::arg("block_size") = 0, py::arg("max_steps") = 0,
              py::arg("timeout") = 0.0, py::arg("attached_potentials") = false,
              py::arg("arbitrary_times") = false)
-        .def("run", &ConfigObject::run, py::kw_only(), py::arg("stats") = false,
-             "Integrate the registered model; results follow first-registration order.")
+        .def("run", &ConfigObject::run, py::kw_only(), py::arg("stats") = false, py::arg("device") = false,
+             "Integrate the registered model; results follow first-registration order.  "
+             "device=True returns torch CUDA tensors that the kernels wrote in place.")
         .def("add", &ConfigObject::add, py::arg("node"),
              "Register force-source edges from ``requires`` to ``node``.")
         .def(

@@ -258,3 +258,36 @@ def test_attached_potentials_move_with_their_group(cuda_device, oracle, method) 
     plain_ref = oracle.integrate_batch(om, oracle.bovy(), stars_state, ts=ts, rtol=1e-10, atol=1e-10)["out"]
     assert np.abs(star_plain - plain_ref).max() < 1e-9
     assert np.abs(star_plain[-1] - star_traj[-1]).max() > 1e-4
+
+
+def test_device_results_stay_on_the_gpu_and_equal_host_results(cuda_device) -> None:
+    """run(device=True): trajectories are torch CUDA tensors written in place
+    by the kernels, bit-identical to run()'s host arrays, exportable through
+    DLPack -- also through a satellite -> stream chain whose origin table is
+    built on the device from the satellite's device trajectory."""
+    import torch
+
+    sat_state = np.array([[1.2, 0.0, 0.05, 0.0, 1.0, 0.02]])
+    rng = np.random.default_rng(12)
+    stars_state = sat_state[0] + np.hstack([rng.normal(0, 0.05, (30, 3)), rng.normal(0, 0.05, (30, 3))])
+
+    def build():
+        gal = dft.background(dft.Potential.bovy())
+        sats = dft.particles(dft.Potential.plummer(0.02, 0.05), sat_state)
+        stars = dft.test_particles(stars_state)
+        sim = dft.Config(method=dft.Method.DOP853, ts=(0.0, 6.0, 31), tolerance=1e-10, attached_potentials=True)
+        sim.add(sats, gal)
+        sim.add(stars, gal, sats)
+        return sim
+
+    host = build().run()
+    dev, stats = build().run(device=True, stats=True)
+    assert dev[1] is None
+    for h, d in zip((host[0], host[2]), (dev[0], dev[2])):
+        assert isinstance(d, torch.Tensor) and d.is_cuda and d.dtype == torch.float64
+        np.testing.assert_array_equal(d.cpu().numpy(), h)
+    assert (stats[2]["status"] == 0).all() and stats[2]["accepted"].min() > 0
+    # zero-copy hand-off to any DLPack consumer
+    capsule = torch.utils.dlpack.to_dlpack(dev[2])
+    back = torch.utils.dlpack.from_dlpack(capsule)
+    assert back.data_ptr() == dev[2].data_ptr()
