@@ -19,6 +19,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "libdrift_b200.so"
 DOPR54, DOP853 = 0, 1
 POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN, POT_MODEL = 0, 1, 2, 3, 4
 MAX_COMPONENTS = 11
+MAX_BATCH = 64  # DRIFT_MAX_BATCH: requests one batched launch carries
 EXACT, FMA = 0, 1
 PLAIN, PERSISTENT, ORDERED = 0, 1, 2
 INITIAL_STEP_SENTINEL = -9999.99

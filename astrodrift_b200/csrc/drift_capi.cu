@@ -371,10 +371,11 @@ int check_batch(const drift_launch *R, int32_t count)
             B.block_size != A.block_size || std::memcmp(&B.potential, &A.potential, sizeof(A.potential)) ||
             B.rtol_ln != A.rtol_ln || B.atol_ln != A.atol_ln || B.dt_one != A.dt_one ||
             B.max_steps != A.max_steps || B.timeout_s != A.timeout_s ||
-            (B.arbitrary_times != 0) != (A.arbitrary_times != 0))
+            (B.arbitrary_times != 0) != (A.arbitrary_times != 0) ||
+            (A.potential.kind == DRIFT_POT_MODEL && B.force_model != A.force_model))
             return fail(DRIFT_ERROR_INVALID_ARGUMENT,
                         "batched requests must share method, precision, schedule, block size, "
-                        "potential, tolerances, first step and limits");
+                        "potential (and force model), tolerances, first step and limits");
     }
     return DRIFT_SUCCESS;
 }
