@@ -258,7 +258,7 @@ struct Dop853Lane {
         }
         der2 = sqrt(der2) / hh;
         double der12 = c_max(fabs(der2), sqrt(dnf));
-        double h1 = root8(0.01 / der12);
+        double h1 = unit_root8(0.01 / der12);
         h = custom_sign(c_min(100.0 * fabs(hh), c_min(fabs(h1), fabs(hmax))), pos_neg);
         reject = 0;
         next = 0;
@@ -365,7 +365,7 @@ struct Dop853Lane {
 
         // fac11 = err^expo1 with expo1 = 1/8; beta = 0 makes the facold
         // factor pow(facold, 0) = 1.
-        double fac11 = root8(err);
+        double fac11 = unit_root8(err);
         double fac = c_max(FACC2, c_min(FACC1, fac11 / SAFE));
         double hnew = h / fac;
 

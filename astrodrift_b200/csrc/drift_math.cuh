@@ -26,6 +26,12 @@
 #include <math.h>
 #include <stdint.h>
 
+// 1: the translation unit reproduces the reference's rounding (see
+// drift_kernels_exact.cu); 0: multiply-add contraction and a-few-ulp powers.
+#ifndef DRIFT_EXACT_ARITH
+#define DRIFT_EXACT_ARITH 1
+#endif
+
 namespace drift {
 
 // Exact product: a * b == hi + lo.
@@ -130,6 +136,60 @@ __device__ __forceinline__ double root8(double x)
     c_l = fma(2.0 * b_h, b_l, c_l);
     double delta = ((c_h - x) + c_l) / x;       // y0^8 / x - 1
     return fma(y0, -0.125 * delta, y0);
+}
+
+// ---- few-ulp variants for the contraction unit -------------------------
+// Without the double-double correction: y = rsqrt(x) refined by two Newton
+// steps is within about an ulp of x^-1/2, and y^3 within a few ulps of
+// x^-3/2; sqrt(x) x and sqrt(sqrt(sqrt(x))) likewise.  The contraction unit
+// already departs from the reference's rounding in every multiply-add, so
+// these save the correction's dozen FP64 instructions per call.
+__device__ __forceinline__ double pow_m1p5_few_ulp(double x)
+{
+    if (__builtin_expect(x > 1e-90 && x < 1e90, 1)) {
+        double y;
+        asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+        y = y * fma(-0.5 * x, y * y, 1.5);
+        y = y * fma(-0.5 * x, y * y, 1.5);
+        return y * (y * y);
+    }
+    return pow_m1p5(x);
+}
+
+__device__ __forceinline__ double pow_1p5_few_ulp(double x)
+{
+    if (in_fast_range(x)) return x * sqrt(x);
+    return pow_1p5(x);
+}
+
+__device__ __forceinline__ double root8_few_ulp(double x) { return sqrt(sqrt(sqrt(x))); }
+
+// The powers as the integrators call them in this translation unit.
+__device__ __forceinline__ double unit_pow_m1p5(double x)
+{
+#if DRIFT_EXACT_ARITH
+    return pow_m1p5(x);
+#else
+    return pow_m1p5_few_ulp(x);
+#endif
+}
+
+__device__ __forceinline__ double unit_pow_1p5(double x)
+{
+#if DRIFT_EXACT_ARITH
+    return pow_1p5(x);
+#else
+    return pow_1p5_few_ulp(x);
+#endif
+}
+
+__device__ __forceinline__ double unit_root8(double x)
+{
+#if DRIFT_EXACT_ARITH
+    return root8(x);
+#else
+    return root8_few_ulp(x);
+#endif
 }
 
 }  // namespace drift

@@ -12,8 +12,9 @@
 //                   exponential cutoff (enclosed-mass force).  In FMA mode
 //                   (DRIFT_EXACT_ARITH 0) the disk and halo use reciprocals
 //                   and rsqrt instead of the reference's divisions.
-// pow(., -1.5) and pow(., 1.5) go through the correctly rounded routines of
-// drift_math.cuh instead of a general pow.
+// pow(., -1.5) and pow(., 1.5) go through the routines of drift_math.cuh
+// instead of a general pow: correctly rounded in the exact unit, within a
+// few ulps in the contraction unit.
 #pragma once
 
 #include "drift_math.cuh"
@@ -44,7 +45,7 @@ struct KeplerGalpy {
         double sin_phi = y / cylindrical_radius;
         double cos_phi = x / cylindrical_radius;
         double radius_squared = cylindrical_radius * cylindrical_radius + z * z;
-        double p = amp * pow_m1p5(radius_squared);
+        double p = amp * unit_pow_m1p5(radius_squared);
         double radial_force = -cylindrical_radius * p;
         // The reference adds (1/R) * sin_phi * phi_torque with phi_torque = 0.
         // For every R >= 0 that term equals sin_phi * 0.0 (a signed zero, or
@@ -81,7 +82,7 @@ struct Plummer {
                                           double &az) const
     {
         double r2 = x * x + y * y + z * z;
-        double ar = -amp * pow_m1p5(r2 + b2);
+        double ar = -amp * unit_pow_m1p5(r2 + b2);
         ax = ar * x;
         ay = ar * y;
         az = ar * z;
@@ -171,7 +172,7 @@ struct Bovy {
             double sqrtz2b2 = sqrt(z2 + mn_b2);
             double apz = mn_a + sqrtz2b2;
             double pyth = apz * apz;
-            double denom = pow_1p5(pyth + r2);
+            double denom = unit_pow_1p5(pyth + r2);
             double ar = -mn_amp * (r / denom);
             dx = ar * (x / r);
             dy = ar * (y / r);
@@ -180,7 +181,7 @@ struct Bovy {
             // a_R x/R == -amp x / D with D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
             double inv_sz = rsqrt(z2 + mn_b2);
             double apz = fma(z2 + mn_b2, inv_sz, mn_a);
-            double m_over_d = -mn_amp * fast_rcp(pow_1p5(fma(apz, apz, r2)));
+            double m_over_d = -mn_amp * unit_pow_m1p5(fma(apz, apz, r2));
             dx = m_over_d * x;
             dy = m_over_d * y;
             dz = m_over_d * z * apz * inv_sz;
