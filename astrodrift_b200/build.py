@@ -42,6 +42,7 @@ CUDA_UNITS = {
     # discrete adjoint (gradients: contraction allowed)
     "drift_adjoint": ["-fmad=true", "-prec-div=true", "-prec-sqrt=true", "-ftz=false"],
     "drift_capi": [],
+    "drift_tuning": [],
     "drift_server": [],
 }
 

@@ -52,7 +52,23 @@ EXPORTED = (
     "drift_origin_table",
     "drift_origin_table_host",
     "drift_force_model_eval",
+    "drift_graph_create",
+    "drift_graph_launch",
+    "drift_graph_destroy",
+    "drift_autotune",
 )
+
+
+class DriftTuning(ctypes.Structure):
+    _fields_ = [
+        ("block_size", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("seconds", ctypes.c_double),
+        ("candidates", ctypes.c_double * 12),
+        ("sample", ctypes.c_int64),
+        ("cached", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
 
 
 class DriftPotential(ctypes.Structure):
@@ -185,6 +201,11 @@ def lib() -> ctypes.CDLL:
         L.drift_origin_table_host.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_int64,
                                               ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
                                               ctypes.c_void_p]
+        L.drift_graph_create.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p,
+                                         ctypes.POINTER(ctypes.c_void_p)]
+        L.drift_graph_launch.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.drift_graph_destroy.argtypes = [ctypes.c_void_p]
+        L.drift_autotune.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_int64, ctypes.POINTER(DriftTuning)]
         L.drift_force_model_eval.argtypes = [ctypes.POINTER(DriftForceModel), ctypes.c_int64, ctypes.c_double,
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         _lib = L
@@ -369,3 +390,35 @@ def integrate_adjoint_device(A: DriftAdjointLaunch, stream: int = 0) -> None:
     """drift_integrate_adjoint on device pointers already stored in ``A``."""
     check(lib().drift_integrate_adjoint(ctypes.byref(A), ctypes.c_void_p(stream)),
           "drift_integrate_adjoint")
+
+
+class Graph:
+    """A captured integration (drift_graph_*): replay() re-runs the launch's
+    whole stream sequence with one call."""
+
+    def __init__(self, L: DriftLaunch, stream: int):
+        self._L = L  # the launch (and what it points to) must outlive the graph
+        self._ptr = ctypes.c_void_p()
+        check(lib().drift_graph_create(ctypes.byref(L), ctypes.c_void_p(stream), ctypes.byref(self._ptr)),
+              "drift_graph_create")
+
+    def replay(self, stream: int) -> None:
+        check(lib().drift_graph_launch(self._ptr, ctypes.c_void_p(stream)), "drift_graph_launch")
+
+    def close(self) -> None:
+        if self._ptr:
+            lib().drift_graph_destroy(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def autotune(L: DriftLaunch, sample: int = 0) -> DriftTuning:
+    """drift_autotune: the fastest block size and schedule for launch L."""
+    t = DriftTuning()
+    check(lib().drift_autotune(ctypes.byref(L), sample, ctypes.byref(t)), "drift_autotune")
+    return t

@@ -281,6 +281,35 @@ int drift_origin_table_host(const drift_force_model *source_model, int64_t n_sou
 int drift_force_model_eval(const drift_force_model *model, int64_t n, double t,
                            const double *xyz, double *acc, void *stream);
 
+/* ---- captured launch graphs (no counterpart in the reference) ----------
+ * drift_graph_create records drift_integrate(launch) on `stream` (not the
+ * legacy default stream) by stream capture: the cursor reset, the ordering
+ * kernels and the integration kernel, with the launch's pointers and values
+ * as they are now.  drift_graph_launch replays that sequence with one call;
+ * change the buffers' contents in place between replays, not the launch. */
+typedef struct drift_graph drift_graph;
+int drift_graph_create(const drift_launch *launch, void *stream, drift_graph **graph);
+int drift_graph_launch(drift_graph *graph, void *stream);
+int drift_graph_destroy(drift_graph *graph);
+
+/* ---- launch autotuner (no counterpart in the reference) -----------------
+ * Times every block size (32, 64, 96, 128) under every schedule on the first
+ * `sample` particles of a device-pointer launch (0: 16384), in scratch
+ * buffers of its own, and returns the fastest.  Results are cached per
+ * workload class (method, precision, potential kind, grid kind, nt and n
+ * rounded to powers of two); `cached` tells whether this call measured.
+ * The launch's own outputs are not written. */
+typedef struct {
+    int32_t block_size;
+    int32_t schedule;
+    double seconds;        /* the winner's time on the sample */
+    double candidates[12]; /* plain, persistent, ordered x block 32..128 */
+    int64_t sample;
+    int32_t cached;
+    int32_t reserved;
+} drift_tuning;
+int drift_autotune(const drift_launch *launch, int64_t sample, drift_tuning *best);
+
 /* ---- discrete adjoint (no counterpart in the reference) ----------------- */
 
 /* Largest number of potential parameters with a gradient:
