@@ -809,7 +809,7 @@ def main() -> None:
         args.e2e_steps = 0
 
     out_bytes = nt * n * 6 * 8
-    e2e_value, e2e_elapsed, e2e_ok = None, 0.0, None
+    e2e_value, e2e_elapsed, e2e_ok, d2h_gbs = None, 0.0, None, None
     if args.e2e_steps > 0:
         lib = capi.lib()
         h_y0, h_out = ctypes.c_void_p(), ctypes.c_void_p()
@@ -837,7 +837,20 @@ def main() -> None:
             e2e_elapsed = reduce_max(e2e_elapsed, dist, dev)
         e2e_value = accepted_all * args.e2e_steps / e2e_elapsed
         e2e_ok = bool(np.array_equal(out_pinned[-1], out_d[-1].cpu().numpy()))
-        del y0_pinned, out_pinned
+        # the copy roofline of this leg: pinned device->host bandwidth of 1 GiB
+        # copies on this box (best of 3, CUDA events)
+        probe = out_d.view(-1)[: (1 << 27)]
+        host_probe = torch.from_numpy(out_pinned.reshape(-1)[: (1 << 27)])
+        d2h = []
+        for _ in range(3):
+            a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a_.record()
+            host_probe.copy_(probe, non_blocking=True)
+            b_.record()
+            torch.cuda.synchronize()
+            d2h.append(probe.numel() * 8 / (a_.elapsed_time(b_) * 1e-3) / 1e9)
+        d2h_gbs = max(d2h)
+        del y0_pinned, out_pinned, host_probe
         lib.drift_host_free(h_y0)
         lib.drift_host_free(h_out)
 
@@ -899,7 +912,12 @@ def main() -> None:
                     "h2d_bytes_per_step": int(y0.nbytes + ts.nbytes),
                     "d2h_bytes_per_step": int(out_bytes + n * (48 + 1 + 4 + 4 + 4)),
                     "ms_per_step": 1e3 * e2e_elapsed / max(args.e2e_steps, 1),
-                    "matches_device_path": e2e_ok},
+                    "matches_device_path": e2e_ok,
+                    "copy_roofline": None if d2h_gbs is None else {
+                        "bound": "pcie_d2h", "peak_gbs": d2h_gbs,
+                        "achieved_gbs": out_bytes * args.e2e_steps / e2e_elapsed / 1e9,
+                        "frac": out_bytes * args.e2e_steps / e2e_elapsed / 1e9 / d2h_gbs,
+                        "peak_source": "pinned 1 GiB device->host copies measured in this run"}},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
