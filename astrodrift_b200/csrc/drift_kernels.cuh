@@ -65,16 +65,23 @@ __device__ __forceinline__ Pot make_pot(const KernelArgs &a, const double *table
     return Pot(a.potential, table);
 }
 template <>
+__device__ __forceinline__ Bovy make_pot<Bovy>(const KernelArgs &a, const double *table)
+{
+    return Bovy(a.potential, table, a.bulge.c);
+}
+template <>
 __device__ __forceinline__ Composite make_pot<Composite>(const KernelArgs &a, const double *table)
 {
-    return Composite(&a.model, table);
+    return Composite(&a.model, table, a.bulge.c);
 }
 
+// Potentials that read the bulge table staged in shared memory.
 template <class Pot>
 __host__ __device__ constexpr bool needs_bulge_table()
 {
     return std::is_same<Pot, Bovy>::value || std::is_same<Pot, Composite>::value;
 }
+
 
 // Launch bounds of the integration kernels: at most DRIFT_MAX_THREADS
 // threads per block, and registers allocated so that DRIFT_MIN_BLOCKS_PER_SM
@@ -87,7 +94,7 @@ __host__ __device__ constexpr bool needs_bulge_table()
 #endif
 
 // Dynamic shared memory per block: the DOP853 rcont parking tile (24
-// doubles per thread, column-major by thread), then the Bovy bulge table.
+// doubles per thread, column-major by thread), then the bulge table.
 __host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
 {
     return (method == DRIFT_DOP853 ? 24 * sizeof(double) * block : 0) +
@@ -103,7 +110,7 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
 {
     static_assert(!TAPE || METHOD == DRIFT_DOP853, "the step tape is recorded by DOP853 only");
     extern __shared__ double smem[];
-    // [park tile (DOP853)][bulge table (Bovy)]
+    // [park tile (DOP853)][bulge table (Bovy, force models)]
     volatile double *park = smem + threadIdx.x;
     double *table = smem + (METHOD == DRIFT_DOP853 ? 24 * blockDim.x : 0);
     if (needs_bulge_table<Pot>()) {

@@ -115,13 +115,18 @@ struct BulgeTable {
     double c[BULGE_TABLE_SIZE];
 };
 
-__device__ __forceinline__ double bulge_lower_gamma(const double *table, double s, double x,
-                                                    double gamma_s)
+// `series` and `table` hold the same coefficients: the series part is read
+// with warp-uniform indices (from the kernel parameter, where the unrolled
+// Horner loop takes them as constant operands), the Taylor pieces with
+// per-lane indices (from shared memory, where differing addresses do not
+// serialise).
+__device__ __forceinline__ double bulge_lower_gamma(const double *table, const double *series, double s,
+                                                    double x, double gamma_s)
 {
     if (x < BULGE_X_SERIES) {
-        double p = table[BULGE_SERIES_DEG];
+        double p = series[BULGE_SERIES_DEG];
 #pragma unroll
-        for (int n = BULGE_SERIES_DEG - 1; n >= 0; --n) p = fma(p, x, table[n]);
+        for (int n = BULGE_SERIES_DEG - 1; n >= 0; --n) p = fma(p, x, series[n]);
         return exp(s * log(x) - x) * p;
     }
     if (x < BULGE_X_CONST) {
@@ -140,11 +145,15 @@ struct Bovy {
     double mn_amp, mn_a, mn_b2;
     double nfw_amp, nfw_a;
     double bulge_s, bulge_rc2, bulge_k, bulge_gamma_s;
-    const double *table;  // BulgeTable staged in shared memory
-    __device__ Bovy(const drift_potential &p, const double *bulge_table)
+    double inv_rc2, inv_nfw_a;  // contraction unit: reciprocals formed once
+    const double *table;   // BulgeTable staged in shared memory
+    const double *series;  // the same table in the kernel's parameter space
+    __device__ Bovy(const drift_potential &p, const double *bulge_table, const double *param_table = nullptr)
         : mn_amp(p.mn_amp), mn_a(p.mn_a), mn_b2(p.mn_b * p.mn_b), nfw_amp(p.nfw_amp),
           nfw_a(p.nfw_a), bulge_s(1.5 - 0.5 * p.bulge_alpha), bulge_rc2(p.bulge_rc * p.bulge_rc),
-          bulge_k(p.bulge_k), bulge_gamma_s(p.bulge_gamma_s), table(bulge_table)
+          bulge_k(p.bulge_k), bulge_gamma_s(p.bulge_gamma_s),
+          inv_rc2(1.0 / (p.bulge_rc * p.bulge_rc)), inv_nfw_a(1.0 / p.nfw_a), table(bulge_table),
+          series(param_table ? param_table : bulge_table)
     {
     }
 
@@ -155,9 +164,15 @@ struct Bovy {
         double bx = 0.0, by = 0.0, bz = 0.0;
         double r2s = x * x + y * y + z * z;
         if (r2s != 0.0) {
+#if DRIFT_EXACT_ARITH
             double r = sqrt(r2s);
-            double g = bulge_lower_gamma(table, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
+            double g = bulge_lower_gamma(table, series, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
             double ar_over_r = -bulge_k * g / (r2s * r);
+#else
+            double inv_r = rsqrt(r2s);
+            double g = bulge_lower_gamma(table, series, bulge_s, r2s * inv_rc2, bulge_gamma_s);
+            double ar_over_r = -bulge_k * g * (inv_r * inv_r * inv_r);
+#endif
             bx = ar_over_r * x;
             by = ar_over_r * y;
             bz = ar_over_r * z;
@@ -200,8 +215,7 @@ struct Bovy {
 #else
             double inv_r = rsqrt(r2);
             double r = r2 * inv_r;
-            double inv_a = fast_rcp(nfw_a);
-            double u = r * inv_a;
+            double u = r * inv_nfw_a;
             double term = log(1. + u) - u * fast_rcp(1.0 + u);
             double ar_over_r = -nfw_amp * term * (inv_r * inv_r * inv_r);
             hx = ar_over_r * x;
