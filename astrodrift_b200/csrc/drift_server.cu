@@ -114,6 +114,8 @@ struct drift_server {
     drift_server_options opts{};
     int device = -1;
     int sm_count = 0;
+    int reserve_sms = 0;         // SMs large batches leave free
+    int64_t small_particles = 0; // batches this small count as small
     size_t budget = 0;
     cudaMemPool_t pool = nullptr;
     std::vector<cudaStream_t> streams;
@@ -181,6 +183,7 @@ struct drift_server {
                 break;
             }
         if (slot < 0 || pending.empty()) return false;
+        slot = -1;  // chosen once the batch's size is known
         Request *head = pending.front();
         auto batch = std::make_unique<Batch>();
         size_t room = budget > bytes_inflight ? budget - bytes_inflight : 0;
@@ -249,6 +252,15 @@ struct drift_server {
                 *o += scratch;
         used += scratch;
 
+        // Small batches run on the high-priority stream 0 and may use every
+        // SM; large ones use the other streams and leave the reserve free.
+        const bool small = particles <= small_particles;
+        if (small && !slot_busy[0]) slot = 0;
+        for (int i = 1; slot < 0 && i < (int)slot_busy.size(); i++)
+            if (!slot_busy[i]) slot = i;
+        if (slot < 0) slot = 0;  // only stream 0 is free
+        const int launch_sms = small ? sm_count : std::max(1, sm_count - reserve_sms);
+
         cudaStream_t s = streams[slot];
         void *dmem = nullptr;
         if (cudaMallocFromPoolAsync(&dmem, used, pool, s) != cudaSuccess) {
@@ -291,7 +303,7 @@ struct drift_server {
             D.workspace = base;
             D.workspace_bytes = scratch;
         }
-        int rc = drift_internal_launch_batch(sm_count, sub.data(), (int32_t)sub.size(), base, s);
+        int rc = drift_internal_launch_batch(launch_sms, sub.data(), (int32_t)sub.size(), base, s);
         for (size_t i = 0; i < batch->pieces.size(); i++) {
             Piece &p = batch->pieces[i];
             const drift_launch &L = p.req->L;
@@ -359,7 +371,9 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
     o.memory_fraction = 0.5;
     o.streams = 4;
     o.max_batch_particles = int64_t(1) << 20;
+    o.sm_reserve_percent = 0;
     if (options) {
+        o.sm_reserve_percent = std::min(std::max(options->sm_reserve_percent, 0), 50);
         if (options->memory_fraction > 0) o.memory_fraction = std::min(options->memory_fraction, 0.95);
         if (options->streams > 0) o.streams = std::min(options->streams, 32);
         if (options->max_batch_particles > 0) o.max_batch_particles = options->max_batch_particles;
@@ -371,6 +385,9 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
         return drift_internal_fail(DRIFT_ERROR_NO_DEVICE, "no CUDA device");
     }
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
+    s->reserve_sms = s->sm_count * o.sm_reserve_percent / 100;
+    // a small batch fits the reserve at 256 particles per SM
+    s->small_particles = std::max<int64_t>(int64_t(s->reserve_sms) * 256, 1);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
         cudaGetLastError();
@@ -390,8 +407,11 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     s->streams.resize(o.streams);
     s->slot_busy.assign(o.streams, false);
-    for (auto &st : s->streams)
-        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+    int lowest = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&lowest, &greatest);
+    for (size_t i = 0; i < s->streams.size(); i++)
+        if (cudaStreamCreateWithPriority(&s->streams[i], cudaStreamNonBlocking, i == 0 ? greatest : lowest) !=
+            cudaSuccess) {
             cudaGetLastError();
             return drift_internal_fail(DRIFT_ERROR_CUDA, "cudaStreamCreate failed");
         }

@@ -23,7 +23,7 @@ class ServerOptions(ctypes.Structure):
         ("memory_fraction", ctypes.c_double),
         ("memory_bytes", ctypes.c_size_t),
         ("streams", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("sm_reserve_percent", ctypes.c_int32),
         ("max_batch_particles", ctypes.c_int64),
     ]
 
@@ -94,9 +94,12 @@ class Request:
 
 class Server:
     def __init__(self, memory_fraction: float = 0.5, memory_bytes: int = 0, streams: int = 4,
-                 max_batch_particles: int = 1 << 20):
+                 max_batch_particles: int = 1 << 20, sm_reserve_percent: int = 0):
+        """sm_reserve_percent: share of the SMs (0 to 50) large batches leave
+        to small ones, which run on the high-priority stream (default none)."""
         opts = ServerOptions(memory_fraction=memory_fraction, memory_bytes=memory_bytes,
-                             streams=streams, max_batch_particles=max_batch_particles)
+                             streams=streams, max_batch_particles=max_batch_particles,
+                             sm_reserve_percent=sm_reserve_percent)
         self._ptr = ctypes.c_void_p()
         capi.check(_lib().drift_server_create(ctypes.byref(opts), ctypes.byref(self._ptr)),
                    "drift_server_create")

@@ -338,7 +338,7 @@ def run_serving(args) -> None:
             retire()
         return time.perf_counter() - t_begin, acc, [lat[i] for i in range(len(reqs))], waits
 
-    with Server(memory_fraction=0.6, streams=args.streams) as srv:
+    with Server(memory_fraction=0.6, streams=args.streams, sm_reserve_percent=args.sm_reserve) as srv:
         t_sat, sat_acc, sat_lat, _ = stream(srv, 0.0)
         print(f"serving: saturated {t_sat:.2f} s", file=sys.stderr, flush=True)
         loads = []
@@ -376,7 +376,7 @@ def run_serving(args) -> None:
         "dtype": "f64",
         "data": "synthetic (seeded request stream)",
         "config": {"workload": "serving", "requests": len(reqs), "particles": n_particles,
-                   "streams": args.streams, "precision": args.precision,
+                   "streams": args.streams, "sm_reserve_percent": args.sm_reserve, "precision": args.precision,
                    "trajectory_cap_bytes": cap_bytes, "result_buffers": args.result_buffers,
                    "seed": args.seed},
         "serial_plain": {"value": serial_acc / t_serial, "seconds": t_serial,
@@ -700,6 +700,8 @@ def main() -> None:
     ap.add_argument("--loads", default="0.5,0.8",
                     help="serving: offered loads (fractions of the saturated capacity) for latency")
     ap.add_argument("--streams", type=int, default=4, help="serving: batches in flight")
+    ap.add_argument("--sm-reserve", type=int, default=0,
+                    help="serving: percent of SMs large batches leave to small ones (default none)")
     ap.add_argument("--trajectory-cap-mib", type=int, default=256,
                     help="serving: largest trajectory of one request")
     ap.add_argument("--result-buffers", type=int, default=16, help="serving: pinned result buffers")

@@ -403,7 +403,11 @@ typedef struct {
     double memory_fraction;      /* of the device's free memory at creation; default 0.5 */
     size_t memory_bytes;         /* absolute budget, overrides the fraction when > 0 */
     int32_t streams;             /* batches in flight; default 4 */
-    int32_t reserved;
+    /* Percent of the SMs (0 to 50) that large batches leave to newly
+     * admitted small ones, which run on the highest-priority stream: bounds
+     * how long a small request waits behind a long one, at the price of the
+     * long one's speed.  Default 0 (none). */
+    int32_t sm_reserve_percent;
     int64_t max_batch_particles; /* particles per launch; default 2^20 */
 } drift_server_options;
 

@@ -57,9 +57,11 @@ def _alone(kw):
     return capi.integrate_host(kw["method"], kw["pot"], kw["y0"], schedule=capi.PLAIN, **args)
 
 
-def test_each_result_is_the_same_alone_and_in_the_mix(cuda_device):
+@pytest.mark.parametrize("reserve", [0, 12, 40])  # percent of the SMs left to small batches
+def test_each_result_is_the_same_alone_and_in_the_mix(cuda_device, reserve):
     mix = _mix()
-    with Server(memory_bytes=96 << 20, streams=3, max_batch_particles=20000) as srv:
+    with Server(memory_bytes=96 << 20, streams=3, max_batch_particles=20000,
+                sm_reserve_percent=reserve) as srv:
         handles = [None] * len(mix)
 
         def submit(idx):
