@@ -167,6 +167,25 @@ def cpu_reference(y0: np.ndarray, ts: np.ndarray, sample: int, threads: int) -> 
             "accepted": int(res["accepted"].sum())}
 
 
+def accuracy_vs_oracle(method: int, pot_name: str, y0: np.ndarray, out: np.ndarray, accepted: np.ndarray,
+                       rtol: float, *, ts=None, t_end=None, nt=None, sample: int = 256) -> dict:
+    """Max relative error per sample and accepted-step agreement of a seeded
+    particle sample against the CPU oracle (the checker; run after timing)."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import oracle
+
+    oracle.build()
+    idx = np.sort(np.random.default_rng(777).choice(len(y0), min(sample, len(y0)), replace=False))
+    opot = {"plummer": oracle.plummer(1.0, 1.0), "kepler": oracle.kepler(1.0), "bovy": oracle.bovy()}[pot_name]
+    kw = dict(ts=ts) if ts is not None else dict(t_end=t_end[idx], nt=nt)
+    ref = oracle.integrate_batch(method, opot, y0[idx], rtol=rtol, atol=rtol, threads=os.cpu_count() or 1, **kw)
+    got = out[:, idx]
+    scale = np.maximum(np.abs(ref["out"]).max(axis=2), 1e-300)
+    err = np.abs(got - ref["out"]).max(axis=2) / scale
+    return {"particles": int(len(idx)), "max_rel_err": float(err.max()), "median_rel_err": float(np.median(err)),
+            "accepted_step_agreement": float((accepted[idx].astype(np.int64) == ref["accepted"]).mean())}
+
+
 def run_reference(args) -> None:
     world, rank, _ = _dist()
     if rank != 0:
@@ -520,6 +539,12 @@ def run_config(args) -> None:
         if rank != 0:
             return
     value = accepted / mean_s
+    acc_sample = None
+    if not args.no_cpu and rank == 0:
+        out_host = out_d.cpu().numpy() if nt * n * 48 < (4 << 30) else None
+        if out_host is not None:
+            acc_sample = accuracy_vs_oracle(method, "kepler" if args.workload == "kepler" else "bovy", y0,
+                                            out_host, acc_per, tol, ts=ts, t_end=t_end, nt=nt)
     plain = None
     if schedule != capi.PLAIN and not args.no_plain and not dist:
         Lp, wsp = make(capi.PLAIN)
@@ -550,6 +575,7 @@ def run_config(args) -> None:
                                "min": int(acc_per.min())},
         "particles_not_ok": int((status != 0).sum()),
         "energy_drift": drift_summary(pot, out_first, out_last),  # rank 0's particles
+        "accuracy": acc_sample,
         "plain_launch": plain,
         "clocks": clocks.summary(),
     }
@@ -794,6 +820,12 @@ def main() -> None:
     from astrodrift_b200.energy import drift_summary
 
     e_drift = drift_summary(capi.plummer(1.0, 1.0), out_d[0].cpu().numpy(), out_d[-1].cpu().numpy())
+    acc_c2 = None
+    if rank == 0 and not args.no_cpu:
+        pick = np.sort(np.random.default_rng(777).choice(n, min(256, n), replace=False))
+        sub_out = out_d[:, torch.from_numpy(pick).to(dev)].cpu().numpy()
+        sub_acc = acc_d.cpu().numpy()[pick]
+        acc_c2 = accuracy_vs_oracle(capi.DOP853, "plummer", y0[pick], sub_out, sub_acc, RTOL, ts=ts)
 
     if dist:
         from astrodrift_b200.sharding import reduce_max, reduce_sum
@@ -909,6 +941,7 @@ def main() -> None:
                              "frac": bytes_alg / mean_launch / 1e9 / hbm_peak, "peak_source": hbm_src},
             "kernel_ms_mean": 1e3 * mean_launch,
             "energy_drift": e_drift,
+            "accuracy": acc_c2,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "accepted steps/s",
                     "h2d_bytes_per_step": int(y0.nbytes + ts.nbytes),
