@@ -63,6 +63,7 @@ class _Spec:
     schedule: int
     tape_steps: int | None
     max_steps: int
+    stride: int = 1
 
 
 def _launch(spec: _Spec, pot, y0, n, out=None, tape=None, tape_steps=0, acc=None, status=None):
@@ -80,7 +81,7 @@ def _launch(spec: _Spec, pot, y0, n, out=None, tape=None, tape_steps=0, acc=None
     L.n_accepted = acc.data_ptr() if acc is not None else None
     L.status = status.data_ptr() if status is not None else None
     if tape is not None:
-        L.tape, L.tape_steps = tape.data_ptr(), tape_steps
+        L.tape, L.tape_steps, L.tape_stride = tape.data_ptr(), tape_steps, spec.stride
     ws = None
     need = capi.query_workspace(L)
     if need:
@@ -115,7 +116,8 @@ class Dop853Trajectory:
                         # size the tape from an untaped pass (same arithmetic, same steps)
                         _launch(spec, pot, y0, n, acc=acc, status=status)
                         steps = max(int(acc.max().item()), 1)
-                    tape = torch.empty((n, steps, 8), dtype=torch.float64, device=dev)
+                    tape = torch.empty((n, capi.tape_doubles(steps, spec.stride)), dtype=torch.float64,
+                                       device=dev)
                     out = torch.empty((spec.nt, n, 6), dtype=torch.float64, device=dev)
                     _launch(spec, pot, y0, n, out=out, tape=tape, tape_steps=steps, acc=acc, status=status)
                     st = status.cpu().numpy()
@@ -145,7 +147,7 @@ class Dop853Trajectory:
                         A.ts = spec.ts.data_ptr()
                     else:
                         A.t_end = spec.t_end.data_ptr()
-                    A.tape, A.tape_steps = tape.data_ptr(), ctx.steps
+                    A.tape, A.tape_steps, A.tape_stride = tape.data_ptr(), ctx.steps, spec.stride
                     A.n_accepted, A.status = acc.data_ptr(), status.data_ptr()
                     A.grad_out, A.grad_y0, A.grad_params = g.data_ptr(), grad_y0.data_ptr(), grad_pp.data_ptr()
                     capi.integrate_adjoint_device(A, torch.cuda.current_stream(dev).cuda_stream)
@@ -162,13 +164,16 @@ class Dop853Trajectory:
 def trajectory(y0, potential: capi.DriftPotential, *, params=None, ts=None, t_end=None,
                t0: float = 0.0, nt: int | None = None, rtol: float = 1e-10, atol: float = 1e-10,
                precision: int = capi.FMA, schedule: int = capi.ORDERED,
-               tape_steps: int | None = None, max_steps: int = 0):
+               tape_steps: int | None = None, max_steps: int = 0, checkpoint_stride: int = 1):
     """DOP853 trajectories (nt, N, 6) on the GPU, differentiable with respect
     to ``y0`` (N, 6) and ``params`` (the potential's PARAM_NAMES values).
 
     ``ts`` is a shared output grid; or ``t_end`` (N,) with ``nt`` gives each
     particle the grid t0..t_end[i].  ``tape_steps`` bounds the accepted steps
-    recorded per particle (default: sized by an untaped pass).  Particles
+    recorded per particle (default: sized by an untaped pass).
+    ``checkpoint_stride`` m > 1 keeps a full state every m steps and every
+    step's size (about 8 + 64/m bytes per step instead of 64); the backward
+    pass recomputes the states in between.  Particles
     that fail (step cap, non-finite state) have NaN samples and NaN
     gradients.
     """
@@ -188,12 +193,14 @@ def trajectory(y0, potential: capi.DriftPotential, *, params=None, ts=None, t_en
     if ts is not None:
         ts_t = as_dev(ts)
         spec = _Spec(potential, ts_t, None, t0, int(ts_t.numel()), rtol, atol, precision, schedule,
-                     tape_steps, max_steps)
+                     tape_steps, max_steps, checkpoint_stride)
     else:
         if t_end is None or nt is None:
             raise ValueError("give ts, or t_end and nt")
         spec = _Spec(potential, None, as_dev(t_end), t0, int(nt), rtol, atol, precision, schedule,
-                     tape_steps, max_steps)
+                     tape_steps, max_steps, checkpoint_stride)
+    if not 1 <= checkpoint_stride <= capi.MAX_TAPE_STRIDE:
+        raise ValueError(f"checkpoint_stride must be in [1, {capi.MAX_TAPE_STRIDE}]")
     if params is not None:
         params = torch.as_tensor(params, dtype=torch.float64)
         if params.numel() != len(PARAM_NAMES[potential.kind]):

@@ -26,6 +26,14 @@ INITIAL_STEP_SENTINEL = -9999.99
 (PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT,
  PARTICLE_TAPE_FULL) = range(6)
 ADJOINT_MAX_PARAMS = 6
+MAX_TAPE_STRIDE = 16
+
+
+def tape_doubles(tape_steps: int, tape_stride: int) -> int:
+    """Doubles of step tape per particle (drift_tape_doubles)."""
+    if tape_stride <= 1:
+        return tape_steps * 8
+    return (tape_steps + tape_stride - 1) // tape_stride * 8 + ((tape_steps + 1) & ~1)
 
 # Every symbol the header declares.
 EXPORTED = (
@@ -144,7 +152,7 @@ class DriftLaunch(ctypes.Structure):
         ("tape_steps", ctypes.c_int64),
         ("force_model", ctypes.POINTER(DriftForceModel)),
         ("arbitrary_times", ctypes.c_int32),
-        ("reserved2", ctypes.c_int32),
+        ("tape_stride", ctypes.c_int32),
     ]
 
 
@@ -165,6 +173,8 @@ class DriftAdjointLaunch(ctypes.Structure):
         ("grad_out", ctypes.c_void_p),
         ("grad_y0", ctypes.c_void_p),
         ("grad_params", ctypes.c_void_p),
+        ("tape_stride", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
     ]
 
 

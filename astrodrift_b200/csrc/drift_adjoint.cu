@@ -205,6 +205,8 @@ struct AdjointArgs {
     const double *t_end;
     const double *tape;
     int64_t tape_steps;
+    int32_t tape_stride;
+    int32_t reserved2;
     const uint32_t *n_accepted;
     const uint8_t *status;
     const double *grad_out;
@@ -238,6 +240,59 @@ __device__ __forceinline__ void stage_vjp(const Jac &jac, const double *zpos, co
     lz[3] = Li[0];
     lz[4] = Li[1];
     lz[5] = Li[2];
+}
+
+// One step's stages from y: stage positions Z[i] (i = 1..13, and 14..16
+// when `dense`), stage derivatives K, and the new state.
+template <class Pot>
+__device__ __forceinline__ void recompute_step(const Pot &pot, const double *y, double h, bool dense,
+                                               double (&K)[17][6], double (&Z)[17][3], double *ynew)
+{
+    double z[6];
+#pragma unroll
+    for (int c = 0; c < 3; c++) Z[1][c] = y[c];
+    rhs(pot, y, K[1]);
+#pragma unroll
+    for (int i = 2; i <= 12; i++) {
+#pragma unroll
+        for (int c = 0; c < 6; c++) {
+            double acc = 0.0;
+#pragma unroll
+            for (int j = 1; j < i; j++)
+                if (acoef(i, j) != 0.0) acc += acoef(i, j) * K[j][c];
+            z[c] = y[c] + h * acc;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) Z[i][c] = z[c];
+        rhs(pot, z, K[i]);
+    }
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+        double acc = 0.0;
+#pragma unroll
+        for (int j = 1; j <= 12; j++)
+            if (bcoef(j) != 0.0) acc += bcoef(j) * K[j][c];
+        ynew[c] = y[c] + h * acc;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) Z[13][c] = ynew[c];
+    if (dense) {
+        rhs(pot, ynew, K[13]);
+#pragma unroll
+        for (int i = 14; i <= 16; i++) {
+#pragma unroll
+            for (int c = 0; c < 6; c++) {
+                double acc = 0.0;
+#pragma unroll
+                for (int j = 1; j < i; j++)
+                    if (acoef(i, j) != 0.0) acc += acoef(i, j) * K[j][c];
+                z[c] = y[c] + h * acc;
+            }
+#pragma unroll
+            for (int c = 0; c < 3; c++) Z[i][c] = z[c];
+            rhs(pot, z, K[i]);
+        }
+    }
 }
 
 template <class Pot, class Jac>
@@ -275,76 +330,21 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_kernel(const __grid_const
         double lk1[6] = {0, 0, 0, 0, 0, 0};  // cotangent of f(y_{n+1}) (the next step's k_1)
         double dp[DRIFT_ADJOINT_MAX_PARAMS] = {0, 0, 0, 0, 0, 0};
         int32_t khi = grid.nt - 1;  // highest sample not yet propagated
-        double y[6];
-        const double *tape = a.tape + pid * a.tape_steps * 8;
+        double y0[6];                // the first step's initial state
 
-        for (int64_t s = nacc - 1; s >= 0; --s) {
-            const double2 *row = reinterpret_cast<const double2 *>(tape + s * 8);
-            double2 v0 = row[0], v1 = row[1], v2 = row[2], v3 = row[3];
-            const double t_old = v0.x, h = v0.y;
-            y[0] = v1.x;
-            y[1] = v1.y;
-            y[2] = v2.x;
-            y[3] = v2.y;
-            y[4] = v3.x;
-            y[5] = v3.y;
+        // Reverse of one accepted step that started at (t_old, y) with size h.
+        auto reverse_step = [&](const double *y, double t_old, double h) {
             // Samples of this step: t_old <= t_k (in the direction of
-            // integration), above the samples of earlier steps.
+            // integration), above the samples of later steps.
             int32_t klo = khi;
             while (klo >= 1 && !(pos_neg * grid.at(klo) < pos_neg * t_old)) klo--;
             const bool dense = khi > klo;
 
-            // ---- recompute the step ----
             double K[17][6];
             double Z[17][3];
-            double z[6];
-#pragma unroll
-            for (int c = 0; c < 3; c++) Z[1][c] = y[c];
-            rhs(pot, y, K[1]);
-#pragma unroll
-            for (int i = 2; i <= 12; i++) {
-#pragma unroll
-                for (int c = 0; c < 6; c++) {
-                    double acc = 0.0;
-#pragma unroll
-                    for (int j = 1; j < i; j++)
-                        if (acoef(i, j) != 0.0) acc += acoef(i, j) * K[j][c];
-                    z[c] = y[c] + h * acc;
-                }
-#pragma unroll
-                for (int c = 0; c < 3; c++) Z[i][c] = z[c];
-                rhs(pot, z, K[i]);
-            }
-            double ynew[6];
-#pragma unroll
-            for (int c = 0; c < 6; c++) {
-                double acc = 0.0;
-#pragma unroll
-                for (int j = 1; j <= 12; j++)
-                    if (bcoef(j) != 0.0) acc += bcoef(j) * K[j][c];
-                ynew[c] = y[c] + h * acc;
-            }
-#pragma unroll
-            for (int c = 0; c < 3; c++) Z[13][c] = ynew[c];
-            if (dense) {
-                rhs(pot, ynew, K[13]);
-#pragma unroll
-                for (int i = 14; i <= 16; i++) {
-#pragma unroll
-                    for (int c = 0; c < 6; c++) {
-                        double acc = 0.0;
-#pragma unroll
-                        for (int j = 1; j < i; j++)
-                            if (acoef(i, j) != 0.0) acc += acoef(i, j) * K[j][c];
-                        z[c] = y[c] + h * acc;
-                    }
-#pragma unroll
-                    for (int c = 0; c < 3; c++) Z[i][c] = z[c];
-                    rhs(pot, z, K[i]);
-                }
-            }
+            double ynew_unused[6];
+            recompute_step(pot, y, h, dense, K, Z, ynew_unused);
 
-            // ---- reverse ----
             double L[17][6];
 #pragma unroll
             for (int i = 1; i <= 16; i++)
@@ -434,11 +434,58 @@ __global__ void __launch_bounds__(ADJ_THREADS) adjoint_kernel(const __grid_const
                 lk1[c] = L[1][c];
             }
             khi = klo;
+        };
+
+        auto load_row = [](const double *row, double &t, double &h, double *y) {
+            const double2 *r = reinterpret_cast<const double2 *>(row);
+            double2 v0 = r[0], v1 = r[1], v2 = r[2], v3 = r[3];
+            t = v0.x;
+            h = v0.y;
+            y[0] = v1.x;
+            y[1] = v1.y;
+            y[2] = v2.x;
+            y[3] = v2.y;
+            y[4] = v3.x;
+            y[5] = v3.y;
+        };
+
+        if (a.tape_stride <= 1) {
+            // every step is a row (t_old, h, y_old)
+            const double *tape = a.tape + pid * a.tape_steps * 8;
+            for (int64_t s = nacc - 1; s >= 0; --s) {
+                double t_old, h;
+                load_row(tape + s * 8, t_old, h, y0);
+                reverse_step(y0, t_old, h);
+            }
+        } else {
+            // checkpoints every m steps: recompute the states between them
+            const int64_t m = a.tape_stride;
+            const int64_t ncp = (a.tape_steps + m - 1) / m;
+            const double *block = a.tape + pid * (ncp * 8 + ((a.tape_steps + 1) & ~int64_t(1)));
+            const double *hs = block + ncp * 8;
+            double ys[DRIFT_MAX_TAPE_STRIDE][6];
+            double tt[DRIFT_MAX_TAPE_STRIDE];
+            for (int64_t cp = (nacc - 1) / m; cp >= 0; --cp) {
+                const int64_t j0 = cp * m;
+                const int cnt = (int)min(m, nacc - j0);
+                double h0;
+                load_row(block + cp * 8, tt[0], h0, ys[0]);
+                for (int q = 0; q + 1 < cnt; q++) {
+                    double K[17][6];
+                    double Z[17][3];
+                    const double hq = hs[j0 + q];
+                    recompute_step(pot, ys[q], hq, false, K, Z, ys[q + 1]);
+                    tt[q + 1] = tt[q] + hq;
+                }
+                for (int q = cnt - 1; q >= 0; q--) reverse_step(ys[q], tt[q], hs[j0 + q]);
+                if (cp == 0)
+                    for (int c = 0; c < 6; c++) y0[c] = ys[0][c];
+            }
         }
         // k_1 of the first step is f(y0) (begin); sample 0 is y0 itself.
         {
             double lz[6];
-            stage_vjp(jac, y, lk1, lz, dp);
+            stage_vjp(jac, y0, lk1, lz, dp);
             const double *g0 = a.grad_out + pid * 6;
 #pragma unroll
             for (int c = 0; c < 6; c++) gy[c] = ly[c] + lz[c] + g0[c];
@@ -483,6 +530,8 @@ extern "C" int drift_integrate_adjoint(const drift_adjoint_launch *A, void *stre
                                    "tape, tape_steps, n_accepted, grad_out and grad_y0 are required");
     if (reinterpret_cast<uintptr_t>(A->tape) % 16)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "the tape must be 16-byte aligned");
+    if (A->tape_stride > DRIFT_MAX_TAPE_STRIDE)
+        return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "tape_stride must be at most 16");
     if (A->block_size != 0 && (A->block_size < 32 || A->block_size > drift::adjoint::ADJ_THREADS ||
                                A->block_size % 32))
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT,
@@ -496,6 +545,7 @@ extern "C" int drift_integrate_adjoint(const drift_adjoint_launch *A, void *stre
     a.t_end = A->t_end;
     a.tape = A->tape;
     a.tape_steps = A->tape_steps;
+    a.tape_stride = A->tape_stride;
     a.n_accepted = A->n_accepted;
     a.status = A->status;
     a.grad_out = A->grad_out;

@@ -231,6 +231,9 @@ int validate(const drift_launch *L, bool device_pointers)
             return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the step tape is recorded by DOP853 only");
         if (L->tape_steps < 1 || L->tape_steps > (int64_t(1) << 40) / std::max<int64_t>(L->n, 1))
             return fail(DRIFT_ERROR_INVALID_ARGUMENT, "tape_steps must be >= 1 (and n * tape_steps <= 2^40)");
+        if (L->tape_stride > DRIFT_MAX_TAPE_STRIDE)
+            return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                        "tape_stride must be at most " + std::to_string(DRIFT_MAX_TAPE_STRIDE));
         if (reinterpret_cast<uintptr_t>(L->tape) % 16)
             return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the tape must be 16-byte aligned");
     }
@@ -273,6 +276,7 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.tape = L->tape;
     a.tape_steps = L->tape_steps;
     a.arbitrary_times = L->arbitrary_times != 0;
+    a.tape_stride = L->tape_stride;
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);

@@ -268,11 +268,12 @@ struct Dop853Lane {
 
     // One step attempt (dop853.rs:425-782).  Returns true when accepted.
     // `park` is this thread's column of a [24][blockDim.x] shared tile.
-    // TAPE: an accepted step also writes (t_old, h, y_old[6]) to tape_row.
+    // TAPE: an accepted step also writes (t_old, h, y_old[6]) to tape_row
+    // (when not NULL) and h to h_slot (when not NULL).
     template <bool TAPE = false, class Out>
     __device__ __forceinline__ bool step(const Pot &pot, const Grid &grid, double rtol,
                                          double atol, Out &out, volatile double *park,
-                                         double *tape_row = nullptr)
+                                         double *tape_row = nullptr, double *h_slot = nullptr)
     {
         using namespace dop853c;
         const int RCONT_STRIDE = blockDim.x;
@@ -372,11 +373,14 @@ struct Dop853Lane {
         if (err <= 1.0) {
             nonfinite_run = 0;
             if (TAPE) {
-                double2 *row = reinterpret_cast<double2 *>(tape_row);
-                row[0] = make_double2(t_old, h);
-                row[1] = make_double2(y[0], y[1]);
-                row[2] = make_double2(y[2], y[3]);
-                row[3] = make_double2(y[4], y[5]);
+                if (tape_row) {
+                    double2 *row = reinterpret_cast<double2 *>(tape_row);
+                    row[0] = make_double2(t_old, h);
+                    row[1] = make_double2(y[0], y[1]);
+                    row[2] = make_double2(y[2], y[3]);
+                    row[3] = make_double2(y[4], y[5]);
+                }
+                if (h_slot) *h_slot = h;
             }
             rhs(pot, t_new, k5, k4);  // FSAL: k4 = f(t_new, y_new)
 

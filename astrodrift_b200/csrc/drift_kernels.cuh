@@ -256,11 +256,21 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
         attempts++;
         bool accepted;
         if (METHOD == DRIFT_DOP853) {
-            if (TAPE)
-                accepted = l853.template step<true>(pot, grid, a.rtol, a.atol, out, park,
-                                                    a.tape + (pid * a.tape_steps + nacc) * 8);
-            else
+            if (TAPE) {
+                double *row, *h_slot = nullptr;
+                if (a.tape_stride <= 1) {
+                    row = a.tape + (pid * a.tape_steps + nacc) * 8;
+                } else {
+                    const int64_t m = a.tape_stride;
+                    const int64_t ncp = (a.tape_steps + m - 1) / m;
+                    double *block = a.tape + pid * (ncp * 8 + ((a.tape_steps + 1) & ~int64_t(1)));
+                    row = (nacc % m == 0) ? block + (nacc / m) * 8 : nullptr;
+                    h_slot = block + ncp * 8 + nacc;
+                }
+                accepted = l853.template step<true>(pot, grid, a.rtol, a.atol, out, park, row, h_slot);
+            } else {
                 accepted = l853.step(pot, grid, a.rtol, a.atol, out, park);
+            }
             if (!accepted && l853.nonfinite_run >= DOP853_NONFINITE_LIMIT) {
                 nrej++;
                 finish(DRIFT_PARTICLE_NONFINITE);

@@ -60,6 +60,7 @@ struct KernelArgs {
     int64_t tape_steps;          // tape rows per particle
     int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
     int32_t arbitrary_times;     // DOPR54: intervals end at ts[i + 1]
+    int32_t tape_stride;         // step tape layout (see drift_launch.tape_stride)
     drift_potential potential;
     BulgeTable bulge;            // Bovy (or a force model with Bovy parts): incomplete gamma table
     drift_force_model model;     // potential.kind == DRIFT_POT_MODEL: the summed force

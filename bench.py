@@ -649,7 +649,8 @@ def run_gradient(args) -> None:
     def step():
         y = y0_d.clone().requires_grad_(True)
         p = torch.tensor(params0, dtype=torch.float64, requires_grad=True)
-        out = adjoint.trajectory(y, pot, params=p, ts=ts, rtol=rtol, atol=rtol, tape_steps=tape_steps)
+        out = adjoint.trajectory(y, pot, params=p, ts=ts, rtol=rtol, atol=rtol, tape_steps=tape_steps,
+                                 checkpoint_stride=args.checkpoint_stride)
         loss = ((out[-1, :, :3] - target_d) ** 2).sum()
         ev = torch.cuda.Event(enable_timing=True)
         ev.record()
@@ -689,10 +690,12 @@ def run_gradient(args) -> None:
         "data": "synthetic (seeded progenitor spray, seeded track)",
         "config": {"workload": "stream-gradient", "particles": n, "potential": "bovy", "method": "DOP853",
                    "rtol": rtol, "t_end": 50.0, "accepted_steps": steps_acc, "tape_rows": tape_steps,
-                   "tape_bytes": n * tape_steps * 64, "l2": "inputs reused; trajectory is 2 samples"},
+                   "checkpoint_stride": args.checkpoint_stride,
+                   "tape_bytes": n * capi.tape_doubles(tape_steps, args.checkpoint_stride) * 8,
+                   "l2": "inputs reused; trajectory is 2 samples"},
         "backward_ms": back,
         "forward_ms": ms - back,
-        "loss": float(loss),
+        "loss": float(loss.detach()),
         "grad_norm_y0": float(y.grad.norm()),
         "grad_params": {k: float(v) for k, v in zip(names, p.grad.tolist())},
         "clocks": clocks.summary(),
@@ -722,6 +725,8 @@ def main() -> None:
                          "configurations; serving: a Poisson request stream; stream-gradient: forward + "
                          "adjoint gradient of a stream-track loss")
     ap.add_argument("--no-plain", action="store_true", help="kepler/bovy: skip the plain-launch pass")
+    ap.add_argument("--checkpoint-stride", type=int, default=1,
+                    help="stream-gradient: adjoint tape checkpoint every m steps (1 = every step)")
     ap.add_argument("--requests", type=int, default=32, help="serving: requests in the stream")
     ap.add_argument("--loads", default="0.5,0.8",
                     help="serving: offered loads (fractions of the saturated capacity) for latency")

@@ -186,10 +186,11 @@ typedef struct {
     uint32_t *n_rejected;  /* (n) rejected steps, or NULL */
     void *workspace;       /* device scratch for the persistent and ordered schedules */
     size_t workspace_bytes;
-    /* DOP853 step tape for drift_integrate_adjoint, or NULL: particle i
-     * records accepted step j as 8 doubles (t_old, h, y_old[6]) at
-     * tape[(i * tape_steps + j) * 8].  Device entry points only; not with
-     * batched launches. */
+    /* DOP853 step tape for drift_integrate_adjoint, or NULL (device entry
+     * points only; not with batched launches).  tape_steps bounds the
+     * accepted steps of one particle; the layout follows tape_stride below
+     * and takes drift_tape_doubles(tape_steps, tape_stride) doubles per
+     * particle. */
     double *tape;
     int64_t tape_steps;
     /* With potential.kind == DRIFT_POT_MODEL: the summed force (see
@@ -201,8 +202,25 @@ typedef struct {
      * may hold arbitrary strictly monotone times.  DOP853's dense output
      * handles arbitrary times either way. */
     int32_t arbitrary_times;
-    int32_t reserved2;
+    /* Step tape layout.  <= 1: every accepted step j of particle i is a row
+     * of 8 doubles (t_old, h, y_old[6]) at tape[(i * tape_steps + j) * 8].
+     * m in 2..DRIFT_MAX_TAPE_STRIDE: checkpoints -- particle i's block starts
+     * at tape + i * drift_tape_doubles(tape_steps, m); step j = c m is a row
+     * (t_old, h, y_old[6]) at block + c * 8, and every step's h sits at
+     * block + ceil(tape_steps / m) * 8 + j.  The adjoint recomputes the
+     * m - 1 states between checkpoints: about 8 + 64 / m bytes per step
+     * instead of 64, for one extra forward step per step. */
+    int32_t tape_stride;
 } drift_launch;
+
+#define DRIFT_MAX_TAPE_STRIDE 16
+
+/* Doubles of step tape per particle for a tape_steps / tape_stride pair. */
+static inline int64_t drift_tape_doubles(int64_t tape_steps, int32_t tape_stride)
+{
+    if (tape_stride <= 1) return tape_steps * 8;
+    return (tape_steps + tape_stride - 1) / tape_stride * 8 + ((tape_steps + 1) & ~(int64_t)1);
+}
 
 /* Library / device information. */
 int drift_abi_version(void);
@@ -339,13 +357,15 @@ typedef struct {
     const double *ts;          /* grid exactly as in the forward launch */
     double t0;
     const double *t_end;
-    const double *tape;        /* the forward launch's tape and tape_steps */
+    const double *tape;        /* the forward launch's tape, tape_steps and tape_stride */
     int64_t tape_steps;
     const uint32_t *n_accepted;/* (n) from the forward launch */
     const uint8_t *status;     /* (n) from the forward launch */
     const double *grad_out;    /* (nt, n, 6) cotangent of the trajectory */
     double *grad_y0;           /* (n, 6) */
     double *grad_params;       /* (n, DRIFT_ADJOINT_MAX_PARAMS), or NULL */
+    int32_t tape_stride;
+    int32_t reserved;
 } drift_adjoint_launch;
 
 int drift_integrate_adjoint(const drift_adjoint_launch *adjoint, void *stream);

@@ -35,7 +35,8 @@ def _pot(name):
     return kind, (capi.bovy() if name == "bovy" else pot)
 
 
-def taped(torch, pot, y0, *, ts=None, t_end=None, nt=None, rtol=1e-10, max_steps=0, tape_steps=None):
+def taped(torch, pot, y0, *, ts=None, t_end=None, nt=None, rtol=1e-10, max_steps=0, tape_steps=None,
+          stride=1):
     """Forward launch with a tape, through the C ABI.  Returns device tensors."""
     dev = torch.device("cuda:0")
     n = len(y0)
@@ -55,7 +56,7 @@ def taped(torch, pot, y0, *, ts=None, t_end=None, nt=None, rtol=1e-10, max_steps
         else:
             L.t_end = grid.data_ptr()
         if tape is not None:
-            L.tape, L.tape_steps = tape.data_ptr(), steps
+            L.tape, L.tape_steps, L.tape_stride = tape.data_ptr(), steps, stride
         ws = torch.zeros(max(capi.query_workspace(L), 8), dtype=torch.uint8, device=dev)
         L.workspace, L.workspace_bytes = ws.data_ptr(), ws.numel()
         capi.integrate_device(L, 0)
@@ -64,10 +65,10 @@ def taped(torch, pot, y0, *, ts=None, t_end=None, nt=None, rtol=1e-10, max_steps
     if tape_steps is None:
         launch()
         tape_steps = max(int(acc.max()), 1)
-    tape = torch.empty((n, tape_steps, 8), dtype=torch.float64, device=dev)
+    tape = torch.empty((n, capi.tape_doubles(tape_steps, stride)), dtype=torch.float64, device=dev)
     launch(tape, tape_steps)
     return dict(y0=y0_d, grid=grid, out=out, acc=acc, status=st, tape=tape, steps=tape_steps, nt=nt,
-                shared=ts is not None)
+                shared=ts is not None, stride=stride)
 
 
 def adjoint_kernel(torch, pot, f, grad_out):
@@ -81,7 +82,7 @@ def adjoint_kernel(torch, pot, f, grad_out):
         A.ts = f["grid"].data_ptr()
     else:
         A.t_end = f["grid"].data_ptr()
-    A.tape, A.tape_steps = f["tape"].data_ptr(), f["steps"]
+    A.tape, A.tape_steps, A.tape_stride = f["tape"].data_ptr(), f["steps"], f["stride"]
     A.n_accepted, A.status = f["acc"].data_ptr(), f["status"].data_ptr()
     A.grad_out, A.grad_y0, A.grad_params = g.data_ptr(), gy.data_ptr(), gp.data_ptr()
     capi.integrate_adjoint_device(A, 0)
@@ -90,7 +91,7 @@ def adjoint_kernel(torch, pot, f, grad_out):
 
 
 def replay_inputs(torch, f, ts=None, t_end=None):
-    tape = f["tape"].cpu()
+    tape = f["tape"].cpu().reshape(f["tape"].shape[0], -1, 8)
     nacc = f["acc"].cpu().numpy().astype(np.int64)
     n, nt = tape.shape[0], f["nt"]
     if ts is not None:
@@ -256,3 +257,42 @@ def test_failed_particles_get_nan_gradients_and_a_full_tape_is_reported(cuda_dev
     assert (f["status"].cpu().numpy() == capi.PARTICLE_TAPE_FULL).all()
     with pytest.raises(RuntimeError, match="tape"):
         adjoint.trajectory(torch.tensor(y0, device="cuda"), pot, ts=ts, tape_steps=3)
+
+
+@pytest.mark.parametrize("stride", [2, 5, 16])
+@pytest.mark.parametrize("name", ["plummer", "bovy"])
+def test_checkpointed_tape_gives_the_same_gradients(cuda_device, name, stride):
+    """A tape with a checkpoint every `stride` steps (every step's h kept)
+    holds 8 + 64/stride bytes per step; the adjoint recomputes the states in
+    between and must return the full tape's gradients."""
+    import torch
+
+    kind, pot = _pot(name)
+    y0 = ics(kind, 40, 70 + kind)
+    t_end = np.random.default_rng(3).uniform(2.0, 9.0, 40)  # step counts not multiples of stride
+    full = taped(torch, pot, y0, t_end=t_end, nt=7)
+    cp = taped(torch, pot, y0, t_end=t_end, nt=7, stride=stride, tape_steps=full["steps"])
+    np.testing.assert_array_equal(cp["out"].cpu().numpy(), full["out"].cpu().numpy())
+    assert cp["tape"].numel() < full["tape"].numel() * (8 + 64 / stride + 16) / 64
+    w = np.random.default_rng(4).normal(size=(7, 40, 6))
+    gy_full, gp_full = adjoint_kernel(torch, pot, full, w)
+    gy_cp, gp_cp = adjoint_kernel(torch, pot, cp, w)
+    assert rel(gy_cp, gy_full) < 1e-10
+    P = len(adjoint.PARAM_NAMES[pot.kind])
+    assert rel(gp_cp[:, :P], gp_full[:, :P]) < 1e-10
+
+
+def test_autograd_function_with_checkpoints(cuda_device):
+    import torch
+
+    kind, pot = _pot("bovy")
+    y0 = torch.tensor(ics(kind, 32, 90), device="cuda")
+    ts = np.linspace(0.0, 6.0, 4)
+    grads = []
+    for stride in (1, 8):
+        y = y0.clone().requires_grad_(True)
+        p = torch.tensor(adjoint.params_of(pot), dtype=torch.float64, requires_grad=True)
+        out = adjoint.trajectory(y, pot, params=p, ts=ts, checkpoint_stride=stride)
+        (out[-1, :, :3] ** 2).sum().backward()
+        grads.append((y.grad.cpu().numpy(), p.grad.numpy()))
+    assert rel(grads[1][0], grads[0][0]) < 1e-10 and rel(grads[1][1], grads[0][1]) < 1e-10
