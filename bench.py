@@ -905,9 +905,13 @@ def main() -> None:
         if world == 1 and not args.no_cpu:
             threads = os.cpu_count() or 1
             r = cpu_reference(y0, ts, args.cpu_sample, threads)
+            one = cpu_reference(y0, ts, max(256, args.cpu_sample // 32), 1)
             cpu = {"value": r["value"], "unit": "accepted steps/s", "cores": threads, "kind": "port",
                    "sample": f"{args.cpu_sample} of the {n} seeded particles, full span and grid "
-                             f"({r['seconds']:.1f} s)"}
+                             f"({r['seconds']:.1f} s)",
+                   "one_core": {"value": one["value"], "cores": 1,
+                                "sample": f"{max(256, args.cpu_sample // 32)} particles ({one['seconds']:.1f} s), "
+                                          "the reference's serial per-particle loop"}}
         line = {
             "metric": "accepted steps/s",
             "value": value,

@@ -197,3 +197,35 @@ def test_device_entry_point_with_device_origin_table(cuda_device, oracle):
                           t0=t0, dt=dt)
     ref = oracle.integrate_batch(1, omodel, y0, ts=ts, rtol=1e-10, atol=1e-10)
     assert rel_err(first, ref["out"]) < REL
+
+
+def test_chunked_host_path_with_moving_sources(cuda_device, oracle):
+    """drift_integrate_host splits large requests into particle chunks; every
+    chunk must see the uploaded origin table."""
+    import torch
+
+    sat, ts, traj = _satellite(oracle)
+    t0, dt, nt = ts[0], ts[1] - ts[0], len(ts)
+    table = oracle.origin_table(oracle.bovy(), traj, t0, dt)
+    y0 = disc(70001, 8)
+    model = capi.force_model([capi.bovy()], [(capi.POT_PLUMMER, 0.02, 0.05, 0, 2)], origins=table.ctypes.data,
+                             n_sources=2, n_segments=nt - 1, t0=t0, dt=dt)
+    got = capi.integrate_host(capi.DOP853, capi.model_potential(), y0, ts=ts, rtol=1e-10, atol=1e-10,
+                              model=model)
+    # the device entry point on a device copy of the same table
+    dev = torch.device("cuda:0")
+    table_d = torch.tensor(table, device=dev)
+    model_d = capi.force_model([capi.bovy()], [(capi.POT_PLUMMER, 0.02, 0.05, 0, 2)],
+                               origins=table_d.data_ptr(), n_sources=2, n_segments=nt - 1, t0=t0, dt=dt)
+    y0_d = torch.tensor(y0, device=dev)
+    ts_d = torch.tensor(ts, device=dev)
+    out_d = torch.empty((nt, len(y0), 6), dtype=torch.float64, device=dev)
+    L = capi.make_launch(capi.DOP853, capi.model_potential(), len(y0), nt, rtol=1e-10, atol=1e-10,
+                         schedule=capi.ORDERED)
+    L.force_model = ctypes.pointer(model_d)
+    L.y0, L.ts, L.out = y0_d.data_ptr(), ts_d.data_ptr(), out_d.data_ptr()
+    ws = torch.zeros(max(capi.query_workspace(L), 8), dtype=torch.uint8, device=dev)
+    L.workspace, L.workspace_bytes = ws.data_ptr(), ws.numel()
+    capi.integrate_device(L, 0)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(got["out"], out_d.cpu().numpy())
