@@ -302,7 +302,7 @@ struct Dopr54Lane {
             q += r * r;
         }
         q = q / 6.0;
-        double powertwo = round(LOG2_085 - 0.1 * log2(q));
+        double powertwo = round(LOG2_085 - 0.1 * unit_log2_for_rounding(q));
         if (powertwo > MAX_STEPCHANGE_POWERTWO)
             powertwo = MAX_STEPCHANGE_POWERTWO;
         else if (powertwo < MIN_STEPCHANGE_POWERTWO)

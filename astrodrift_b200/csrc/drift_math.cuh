@@ -164,6 +164,28 @@ __device__ __forceinline__ double pow_1p5_few_ulp(double x)
 
 __device__ __forceinline__ double root8_few_ulp(double x) { return sqrt(sqrt(sqrt(x))); }
 
+// log2(q) for the DOPR54 controller, whose result is only rounded to an
+// integer after scaling by 0.1: in the contraction unit the exponent plus a
+// single-precision log2 of the mantissa in [1, 2) (absolute error ~1e-7,
+// which moves the rounding only when the argument lies that close to a
+// half-integer).  0 -> -inf, NaN -> NaN, +inf -> +inf as log2.
+__device__ __forceinline__ double log2_for_rounding_few_ulp(double q)
+{
+    if (!(q > 0.0) || isinf(q)) return log2(q);
+    int e;
+    const double m = 2.0 * frexp(q, &e);  // q = m 2^(e-1), m in [1, 2)
+    return (double)(e - 1) + (double)__log2f((float)m);
+}
+
+__device__ __forceinline__ double unit_log2_for_rounding(double q)
+{
+#if DRIFT_EXACT_ARITH
+    return log2(q);
+#else
+    return log2_for_rounding_few_ulp(q);
+#endif
+}
+
 // The powers as the integrators call them in this translation unit.
 __device__ __forceinline__ double unit_pow_m1p5(double x)
 {

@@ -41,6 +41,7 @@ struct KeplerGalpy {
     __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
+#if DRIFT_EXACT_ARITH
         double cylindrical_radius = sqrt(x * x + y * y);
         double sin_phi = y / cylindrical_radius;
         double cos_phi = x / cylindrical_radius;
@@ -53,6 +54,17 @@ struct KeplerGalpy {
         ax = cos_phi * radial_force - sin_phi * 0.0;
         ay = sin_phi * radial_force + cos_phi * 0.0;
         az = -z * p;
+#else
+        // cos(phi) (-R p) = -x p wherever R > 0: no square root or division
+        // on the dependency chain; on the z axis (R = 0) the cylindrical
+        // form's NaN is kept.
+        const double R2 = x * x + y * y;
+        const double p = amp * unit_pow_m1p5(fma(z, z, R2));
+        const double nan_if_axis = R2 > 0.0 ? 1.0 : __longlong_as_double(0x7ff8000000000000LL);
+        ax = -x * p * nan_if_axis;
+        ay = -y * p * nan_if_axis;
+        az = -z * p;
+#endif
     }
 };
 
