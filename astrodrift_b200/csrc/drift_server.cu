@@ -384,6 +384,25 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
         cudaGetLastError();
         return drift_internal_fail(DRIFT_ERROR_NO_DEVICE, "no CUDA device");
     }
+    if (options && options->select_device) {
+        int count = 0;
+        if (cudaGetDeviceCount(&count) != cudaSuccess || options->device < 0 || options->device >= count) {
+            cudaGetLastError();
+            return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "no such CUDA device");
+        }
+        s->device = options->device;
+    }
+    // every call below, and the scheduler thread, work on the server's device
+    int caller_device = -1;
+    cudaGetDevice(&caller_device);
+    cudaSetDevice(s->device);
+    struct RestoreDevice {
+        int d;
+        ~RestoreDevice()
+        {
+            if (d >= 0) cudaSetDevice(d);
+        }
+    } restore{caller_device};
     cudaDeviceGetAttribute(&s->sm_count, cudaDevAttrMultiProcessorCount, s->device);
     s->reserve_sms = s->sm_count * o.sm_reserve_percent / 100;
     // a small batch fits the reserve at 256 particles per SM
@@ -475,6 +494,10 @@ int drift_server_stats_get(drift_server *s, drift_server_stats *out)
     out->requests_pending = s->pending.size();
     out->batches_in_flight = s->inflight.size();
     out->bytes_in_flight = s->bytes_inflight;
+    out->bytes_pending = 0;
+    for (const Request *r : s->pending) out->bytes_pending += piece_bytes(r->L, r->L.n - r->admitted);
+    out->device = s->device;
+    out->reserved = 0;
     return DRIFT_SUCCESS;
 }
 

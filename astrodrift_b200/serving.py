@@ -25,6 +25,8 @@ class ServerOptions(ctypes.Structure):
         ("streams", ctypes.c_int32),
         ("sm_reserve_percent", ctypes.c_int32),
         ("max_batch_particles", ctypes.c_int64),
+        ("select_device", ctypes.c_int32),
+        ("device", ctypes.c_int32),
     ]
 
 
@@ -32,7 +34,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(name, ctypes.c_uint64) for name in (
         "requests_submitted", "requests_completed", "requests_pending", "particles_completed",
         "batches_launched", "pieces_launched", "batches_in_flight", "bytes_to_device",
-        "bytes_to_host", "memory_budget", "bytes_in_flight", "peak_bytes_in_flight")]
+        "bytes_to_host", "memory_budget", "bytes_in_flight", "peak_bytes_in_flight",
+        "bytes_pending")] + [("device", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 def _lib():
@@ -94,15 +97,21 @@ class Request:
 
 class Server:
     def __init__(self, memory_fraction: float = 0.5, memory_bytes: int = 0, streams: int = 4,
-                 max_batch_particles: int = 1 << 20, sm_reserve_percent: int = 0):
+                 max_batch_particles: int = 1 << 20, sm_reserve_percent: int = 0,
+                 device: int | None = None):
         """sm_reserve_percent: share of the SMs (0 to 50) large batches leave
-        to small ones, which run on the high-priority stream (default none)."""
+        to small ones, which run on the high-priority stream (default none).
+        ``device``: the CUDA device index the server runs on (default: the
+        current device)."""
         opts = ServerOptions(memory_fraction=memory_fraction, memory_bytes=memory_bytes,
                              streams=streams, max_batch_particles=max_batch_particles,
-                             sm_reserve_percent=sm_reserve_percent)
+                             sm_reserve_percent=sm_reserve_percent,
+                             select_device=int(device is not None),
+                             device=int(device) if device is not None else 0)
         self._ptr = ctypes.c_void_p()
         capi.check(_lib().drift_server_create(ctypes.byref(opts), ctypes.byref(self._ptr)),
                    "drift_server_create")
+        self.device_index = self.stats()["device"]
 
     def submit(self, method, pot, y0, *, ts=None, t_end=None, nt=None, t0=0.0, rtol=1e-12,
                atol=1e-12, precision=capi.EXACT, schedule=capi.ORDERED, out=None,
@@ -151,6 +160,104 @@ class Server:
         if self._ptr:
             _lib().drift_server_destroy(self._ptr)
             self._ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def request_bytes(n: int, nt: int, *, shared_grid: bool = True, want_out: bool = True) -> int:
+    """Device bytes a whole request of ``n`` particles and ``nt`` samples
+    needs on a server (the sum the server's admission reserves for it: state,
+    grid, trajectory, final state and per-particle counters, each rounded to
+    256 bytes)."""
+    def up(b):
+        return (b + 255) // 256 * 256
+    b = up(n * 48) + up(nt * 8 if shared_grid else n * 8) + up(n * 48) + up(n) + 3 * up(n * 4)
+    if want_out:
+        b += up(nt * n * 48)
+    return b
+
+
+def route(free_bytes, pending_requests, need: int) -> int:
+    """Index of the server a request needing ``need`` device bytes goes to.
+
+    The server with the most free device memory (budget minus bytes in
+    flight minus bytes queued) wins; ties go to the one with fewer queued
+    requests, then the lower index.  A request larger than every server's
+    free memory still goes to the freest one, which runs it in particle
+    chunks as memory frees up."""
+    if not free_bytes:
+        raise ValueError("no servers")
+    if len(free_bytes) != len(pending_requests):
+        raise ValueError("free_bytes and pending_requests differ in length")
+    del need  # the ranking does not depend on the request's size
+    return min(range(len(free_bytes)), key=lambda i: (-int(free_bytes[i]), int(pending_requests[i]), i))
+
+
+class Router:
+    """Whole requests to one of several servers, typically one per GPU of a
+    node, by free device memory.
+
+        with Router.on_devices([0, 1, 2, 3], memory_fraction=0.5) as rt:
+            req = rt.submit(capi.DOP853, capi.plummer(), y0, ts=ts)
+            res = req.wait()       # res["device"] is the GPU that ran it
+
+    A request never splits across servers: its particles stay on one GPU,
+    so its results equal drift_integrate_host's on that GPU."""
+
+    def __init__(self, servers):
+        self.servers = list(servers)
+        if not self.servers:
+            raise ValueError("a router needs at least one server")
+        self.routed = [0] * len(self.servers)
+
+    @classmethod
+    def on_devices(cls, devices=None, **server_kwargs) -> "Router":
+        """One server per CUDA device index in ``devices`` (default: every
+        visible device)."""
+        if devices is None:
+            import torch
+
+            devices = range(torch.cuda.device_count())
+        servers = []
+        try:
+            for d in devices:
+                servers.append(Server(device=int(d), **server_kwargs))
+        except Exception:
+            for s in servers:
+                s.close()
+            raise
+        return cls(servers)
+
+    def pick(self, need: int) -> int:
+        free, queued = [], []
+        for s in self.servers:
+            st = s.stats()
+            used = st["bytes_in_flight"] + st["bytes_pending"]
+            free.append(max(st["memory_budget"] - used, 0))
+            queued.append(st["requests_pending"])
+        return route(free, queued, need)
+
+    def submit(self, method, pot, y0, *, ts=None, t_end=None, nt=None, want_out=True, **kwargs) -> Request:
+        n = int(np.asarray(y0).size // 6)
+        samples = len(ts) if ts is not None else int(nt)
+        i = self.pick(request_bytes(n, samples, shared_grid=ts is not None, want_out=want_out))
+        self.routed[i] += 1
+        server = self.servers[i]
+        req = server.submit(method, pot, y0, ts=ts, t_end=t_end, nt=nt, want_out=want_out, **kwargs)
+        req.arrays["device"] = server.device_index
+        req.arrays["server"] = i
+        return req
+
+    def stats(self) -> list[dict]:
+        return [s.stats() for s in self.servers]
+
+    def close(self):
+        for s in self.servers:
+            s.close()
 
     def __enter__(self):
         return self

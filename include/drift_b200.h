@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DRIFT_ABI_VERSION 3
+#define DRIFT_ABI_VERSION 4
 
 /* Sentinel that asks DOPR54 for galpy's RK4 initial-step estimate
  * (src/integrators/galpy/mod.rs:8). */
@@ -429,6 +429,10 @@ typedef struct {
      * long one's speed.  Default 0 (none). */
     int32_t sm_reserve_percent;
     int64_t max_batch_particles; /* particles per launch; default 2^20 */
+    /* select_device != 0: the server's pool, streams and kernels live on
+     * CUDA device `device`; 0 (default): on the caller's current device. */
+    int32_t select_device;
+    int32_t device;
 } drift_server_options;
 
 typedef struct {
@@ -437,6 +441,9 @@ typedef struct {
     uint64_t batches_launched, pieces_launched, batches_in_flight;
     uint64_t bytes_to_device, bytes_to_host;
     uint64_t memory_budget, bytes_in_flight, peak_bytes_in_flight;
+    uint64_t bytes_pending;  /* device bytes the queued, not yet admitted particles need */
+    int32_t device;          /* the server's CUDA device */
+    int32_t reserved;
 } drift_server_stats;
 
 int drift_server_create(const drift_server_options *options, drift_server **server);

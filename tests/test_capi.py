@@ -10,7 +10,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from astrodrift_b200 import capi
+from astrodrift_b200 import capi, serving
 
 HEADER = Path(__file__).resolve().parent.parent / "include" / "drift_b200.h"
 
@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_messages():
     lib = capi.lib()
-    assert lib.drift_abi_version() == 3
+    assert lib.drift_abi_version() == 4
     assert lib.drift_result_string(0) == b"success"
     assert lib.drift_result_string(1) == b"invalid argument"
 
@@ -44,7 +44,8 @@ def test_struct_layout_matches_header(tmp_path):
     lines = []
     structs = (("drift_potential", capi.DriftPotential), ("drift_launch", capi.DriftLaunch),
                ("drift_adjoint_launch", capi.DriftAdjointLaunch), ("drift_source_group", capi.DriftSourceGroup),
-               ("drift_force_model", capi.DriftForceModel))
+               ("drift_force_model", capi.DriftForceModel), ("drift_server_options", serving.ServerOptions),
+               ("drift_server_stats", serving.ServerStats))
     for struct_name, cls in structs:
         lines.append(f'printf("{struct_name} %zu\\n", sizeof({struct_name}));')
         for field, _ in cls._fields_:

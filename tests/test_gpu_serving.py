@@ -112,3 +112,56 @@ def test_close_with_requests_in_flight_returns(cuda_device):
     srv.close()  # batches in flight finish; requests not yet admitted are cancelled
     with pytest.raises(RuntimeError, match="closed"):
         hs[-1].wait(timeout=1)
+
+
+def test_server_on_an_explicit_device_and_a_missing_one(cuda_device):
+    with Server(memory_bytes=32 << 20, device=0) as srv:
+        assert srv.device_index == 0
+        assert srv.stats()["device"] == 0
+    with pytest.raises(RuntimeError, match="no such CUDA device"):
+        Server(device=1 << 20)
+
+
+def test_router_sends_each_request_whole_to_the_freest_server(cuda_device):
+    """Two servers on the same GPU with different budgets: the first request
+    goes to the larger one, every request's result equals the one it gets
+    alone, and the queued bytes the servers report match the host estimate."""
+    from astrodrift_b200.serving import Router, request_bytes
+
+    mix = _mix(seed=3, count=12)
+    servers = [Server(memory_bytes=48 << 20, streams=2), Server(memory_bytes=160 << 20, streams=2)]
+    with Router(servers) as rt:
+        handles = []
+        for kw in mix:
+            args = {k: v for k, v in kw.items() if k not in ("method", "pot", "y0")}
+            handles.append(rt.submit(kw["method"], kw["pot"], kw["y0"], **args))
+        assert handles[0].arrays["server"] == 1
+        results = [h.wait(timeout=600) for h in handles]
+        assert sum(rt.routed) == len(mix)
+        for st in rt.stats():
+            assert st["bytes_pending"] == 0 and st["requests_pending"] == 0
+    for kw, res in zip(mix, results):
+        ref = _alone(kw)
+        np.testing.assert_array_equal(res["out"], ref["out"])
+        np.testing.assert_array_equal(res["status"], ref["status"])
+        assert res["device"] == 0
+
+
+def test_queued_bytes_match_the_host_estimate(cuda_device):
+    from astrodrift_b200.serving import request_bytes
+
+    rng = np.random.default_rng(5)
+    n_long, n_wait, nt = 60000, 3000, 9
+    y_long = np.hstack([rng.uniform(0.5, 2.0, (n_long, 3)), rng.normal(0, 0.3, (n_long, 3))])
+    y_wait = np.hstack([rng.uniform(0.5, 2.0, (n_wait, 3)), rng.normal(0, 0.3, (n_wait, 3))])
+    ts = np.linspace(0.0, 40.0, nt)
+    with Server(memory_bytes=512 << 20, streams=1) as srv:
+        a = srv.submit(capi.DOP853, capi.bovy(), y_long, ts=ts, rtol=1e-12, atol=1e-12)
+        # a different tolerance cannot join the first batch, so it waits for the one stream
+        b = srv.submit(capi.DOP853, capi.bovy(), y_wait, ts=ts, rtol=1e-11, atol=1e-11)
+        st = srv.stats()
+        if st["requests_pending"] == 1 and st["batches_in_flight"] == 1:
+            assert st["bytes_pending"] == request_bytes(n_wait, nt)
+        a.wait(timeout=600)
+        b.wait(timeout=600)
+        assert srv.stats()["bytes_pending"] == 0
