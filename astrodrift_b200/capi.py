@@ -49,6 +49,7 @@ EXPORTED = (
     "drift_galpy_dopr54",
     "drift_galpy_dop853",
     "drift_force",
+    "drift_force_precision",
     "drift_integrate_noalloc",
     "drift_integrate_batch",
     "drift_server_create",
@@ -202,6 +203,8 @@ def lib() -> ctypes.CDLL:
         L.drift_galpy_dop853.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 2 + [ctypes.c_void_p]
         L.drift_force.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int64, ctypes.c_void_p,
                                   ctypes.c_void_p, ctypes.c_void_p]
+        L.drift_force_precision.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int32, ctypes.c_int64,
+                                            ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
         L.drift_integrate_noalloc.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
         L.drift_integrate_batch.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_int32, ctypes.c_void_p]
         L.drift_integrate_adjoint.argtypes = [ctypes.POINTER(DriftAdjointLaunch), ctypes.c_void_p]
@@ -385,10 +388,12 @@ def integrate_batch_device(launches: list, stream: int = 0) -> None:
           "drift_integrate_batch")
 
 
-def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream: int = 0) -> None:
-    """drift_force on device pointers."""
-    check(lib().drift_force(ctypes.byref(pot), n, ctypes.c_void_p(xyz_ptr), ctypes.c_void_p(acc_ptr),
-                            ctypes.c_void_p(stream)), "drift_force")
+def force_device(pot: DriftPotential, n: int, xyz_ptr: int, acc_ptr: int, stream: int = 0,
+                 precision: int = EXACT) -> None:
+    """drift_force_precision on device pointers."""
+    check(lib().drift_force_precision(ctypes.byref(pot), precision, n, ctypes.c_void_p(xyz_ptr),
+                                      ctypes.c_void_p(acc_ptr), ctypes.c_void_p(stream)),
+          "drift_force_precision")
 
 
 def exported_symbols() -> dict[str, bool]:

@@ -632,8 +632,16 @@ int drift_integrate_batch(const drift_launch *requests, int32_t count, void *str
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream)
 {
+    return drift_force_precision(potential, DRIFT_PRECISION_EXACT, n, xyz, acc, stream);
+}
+
+int drift_force_precision(const drift_potential *potential, int32_t precision, int64_t n,
+                          const double *xyz, double *acc, void *stream)
+{
     if (!potential || !xyz || !acc || n < 0)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_force: NULL pointer or negative n");
+    if (precision != DRIFT_PRECISION_EXACT && precision != DRIFT_PRECISION_FMA)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown precision");
     const int k = potential->kind;
     if (k < DRIFT_POT_KEPLER || k > DRIFT_POT_KEPLER_CARTESIAN)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown potential kind");
@@ -645,8 +653,11 @@ int drift_force(const drift_potential *potential, int64_t n, const double *xyz, 
     drift::BulgeTable table;
     std::memset(&table, 0, sizeof(table));
     if (k == DRIFT_POT_BOVY) drift::fill_bulge_table(1.5 - 0.5 * potential->bulge_alpha, &table);
-    DRIFT_CUDA_TRY(drift::force_exact(*potential, n, xyz, acc, table, (int)blocks,
-                                      static_cast<cudaStream_t>(stream)),
+    DRIFT_CUDA_TRY(precision == DRIFT_PRECISION_FMA
+                       ? drift::force_fma(*potential, n, xyz, acc, table, (int)blocks,
+                                          static_cast<cudaStream_t>(stream))
+                       : drift::force_exact(*potential, n, xyz, acc, table, (int)blocks,
+                                            static_cast<cudaStream_t>(stream)),
                    "force kernel launch");
     return DRIFT_SUCCESS;
 }

@@ -362,13 +362,24 @@ struct Dop853Lane {
         }
         double deno = err + 0.01 * err2;
         if (deno <= 0.0) deno = 1.0;
+#if DRIFT_EXACT_ARITH
         err = fabs(h) * err * sqrt(1.0 / (deno * 6.0));
+#else
+        // the contraction unit divides by reciprocal estimates (a few ulps)
+        err = fabs(h) * err * rsqrt(deno * 6.0);
+#endif
 
         // fac11 = err^expo1 with expo1 = 1/8; beta = 0 makes the facold
         // factor pow(facold, 0) = 1.
         double fac11 = unit_root8(err);
+#if DRIFT_EXACT_ARITH
         double fac = c_max(FACC2, c_min(FACC1, fac11 / SAFE));
         double hnew = h / fac;
+#else
+        constexpr double INV_SAFE = 1.0 / SAFE;
+        double fac = c_max(FACC2, c_min(FACC1, fac11 * INV_SAFE));
+        double hnew = h * fast_rcp(fac);
+#endif
 
         if (err <= 1.0) {
             nonfinite_run = 0;
@@ -443,10 +454,17 @@ struct Dop853Lane {
             t_cur = t_new;
 
             // Dense output of every requested time strictly before t_current.
+#if !DRIFT_EXACT_ARITH
+            const double inv_h = fast_rcp(h);
+#endif
             while (next < grid.nt - 1) {
                 double tk = grid.at(next + 1);
                 if (!(pos_neg * tk < pos_neg * t_cur)) break;
+#if DRIFT_EXACT_ARITH
                 double s = (tk - t_old) / h;
+#else
+                double s = (tk - t_old) * inv_h;
+#endif
                 double s1 = 1.0 - s;
                 double yy[6];
 #pragma unroll
@@ -467,7 +485,11 @@ struct Dop853Lane {
             h = hnew;
             return true;
         }
+#if DRIFT_EXACT_ARITH
         hnew = h / c_min(FACC1, fac11 / SAFE);
+#else
+        hnew = h * fast_rcp(c_min(FACC1, fac11 * INV_SAFE));
+#endif
         reject = 1;
         nonfinite_run = isfinite(err) ? 0 : nonfinite_run + 1;
         h = hnew;

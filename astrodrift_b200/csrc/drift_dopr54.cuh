@@ -109,7 +109,11 @@ struct Dopr54Lane {
             double v = fabs(y[i]);
             if (v > m) m = v;
         }
+#if DRIFT_EXACT_ARITH
         return 1.0 / (tol.e_atol + tol.e_rtol * m);
+#else
+        return fast_rcp(tol.e_atol + tol.e_rtol * m);
+#endif
     }
 
     // rk4_onestep (dopr54.rs:135-208): yn1 += RK4 increment of step dt.
@@ -301,7 +305,11 @@ struct Dopr54Lane {
             double r = yerr[i] * isc;
             q += r * r;
         }
+#if DRIFT_EXACT_ARITH
         q = q / 6.0;
+#else
+        q = q * (1.0 / 6.0);
+#endif
         double powertwo = round(LOG2_085 - 0.1 * unit_log2_for_rounding(q));
         if (powertwo > MAX_STEPCHANGE_POWERTWO)
             powertwo = MAX_STEPCHANGE_POWERTWO;
@@ -318,8 +326,12 @@ struct Dopr54Lane {
             to += h;
             advanced = true;
         }
-        // dt * pow(2, powertwo): an exact power-of-two scaling (NaN stays NaN).
-        dt_one = (powertwo == powertwo) ? scalbn(h, (int)powertwo) : powertwo;
+        // dt * pow(2, powertwo) with powertwo an integer in [-3, 3]: a
+        // product with an exact power of two, which rounds (subnormal results)
+        // and overflows exactly as scalbn does.  NaN stays NaN.
+        dt_one = (powertwo == powertwo)
+                     ? h * __longlong_as_double((long long)(1023 + (int)powertwo) << 52)
+                     : powertwo;
         close_intervals(grid, out);
         return advanced;
     }

@@ -85,6 +85,8 @@ cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned
                         uint32_t *order, int sm_count, cudaStream_t stream);
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
                         const BulgeTable &bt, int grid, cudaStream_t stream);
+cudaError_t force_fma(const drift_potential &p, int64_t n, const double *xyz, double *acc,
+                      const BulgeTable &bt, int grid, cudaStream_t stream);
 // Force model at time t (exact unit).
 cudaError_t model_force_exact(const drift_force_model &m, const BulgeTable &bt, double t, int64_t n,
                               const double *xyz, double *acc, int grid, cudaStream_t stream);

@@ -69,6 +69,8 @@ __device__ __forceinline__ double fast_rcp(double x)
 }
 
 // x^(3/2), rounded to nearest (pow(x, 1.5) semantics for x >= 0).
+static __device__ __noinline__ double pow_1p5_rare(double x);
+
 __device__ __forceinline__ double pow_1p5(double x)
 {
     if (in_fast_range(x)) {
@@ -76,6 +78,12 @@ __device__ __forceinline__ double pow_1p5(double x)
         pow_1p5_dd(x, hi, lo);
         return hi + lo;
     }
+    return pow_1p5_rare(x);
+}
+
+// Arguments outside [1e-200, 1e200], out of line like pow_m1p5_rare.
+static __device__ __noinline__ double pow_1p5_rare(double x)
+{
     if (x == 0.0) return 0.0;
     if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);  // NaN
     if (isinf(x)) return x;
@@ -111,15 +119,24 @@ __device__ __forceinline__ double pow_m1p5_core(double x)
 
 // x^(-3/2), rounded to nearest (pow(x, -1.5) semantics, including the
 // special values: +-0 -> +inf, +inf -> +0, x < 0 -> NaN).
-__device__ __forceinline__ double pow_m1p5(double x)
+//
+// The arguments outside (1e-90, 1e90) take an out-of-line path: the force
+// is inlined at every stage of a step, and one shared copy of the rescaling
+// keeps it out of each copy's instruction stream.
+static __device__ __noinline__ double pow_m1p5_rare(double x)
 {
-    if (__builtin_expect(x > 1e-90 && x < 1e90, 1)) return pow_m1p5_core(x);
     if (x == 0.0) return __longlong_as_double(0x7ff0000000000000LL);  // +inf
     if (!(x >= 0.0)) return __longlong_as_double(0x7ff8000000000000LL);
     if (isinf(x)) return 0.0;
     int k = (ilogb(x)) / 2;
     double m = scalbn(x, -2 * k);
     return scalbn(pow_m1p5_core(m), -3 * k);
+}
+
+__device__ __forceinline__ double pow_m1p5(double x)
+{
+    if (__builtin_expect(x > 1e-90 && x < 1e90, 1)) return pow_m1p5_core(x);
+    return pow_m1p5_rare(x);
 }
 
 // x^(1/8), rounded to nearest (pow(x, 0.125) semantics for the values the
@@ -147,19 +164,23 @@ __device__ __forceinline__ double root8(double x)
 __device__ __forceinline__ double pow_m1p5_few_ulp(double x)
 {
     if (__builtin_expect(x > 1e-90 && x < 1e90, 1)) {
+        // y = x^-1/2 (1 + d) from the hardware estimate; with
+        // e = 1 - x y^2 = 1 - (1 + d)^2 the power is
+        // x^-3/2 = y^3 (1 - e)^-3/2 = y^3 (1 + 3/2 e + 15/8 e^2 + 35/16 e^3 + O(e^4)),
+        // one correction of depth 6 instead of two Newton steps and a cube.
         double y;
         asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-        y = y * fma(-0.5 * x, y * y, 1.5);
-        y = y * fma(-0.5 * x, y * y, 1.5);
-        return y * (y * y);
+        const double e = fma(-x * y, y, 1.0);
+        const double y3 = y * (y * y);
+        return fma(y3, e * fma(fma(2.1875, e, 1.875), e, 1.5), y3);
     }
-    return pow_m1p5(x);
+    return pow_m1p5_rare(x);
 }
 
 __device__ __forceinline__ double pow_1p5_few_ulp(double x)
 {
     if (in_fast_range(x)) return x * sqrt(x);
-    return pow_1p5(x);
+    return pow_1p5_rare(x);
 }
 
 __device__ __forceinline__ double root8_few_ulp(double x) { return sqrt(sqrt(sqrt(x))); }

@@ -277,6 +277,11 @@ int drift_integrate_batch(const drift_launch *requests, int32_t count, void *str
  * through its Potential trait (shared/src/potential.rs:41-44). */
 int drift_force(const drift_potential *potential, int64_t n, const double *xyz, double *acc,
                 void *stream);
+/* The same, rounded as the chosen precision unit's integrators round
+ * (drift_precision): DRIFT_PRECISION_FMA gives the contraction unit's force,
+ * with its few-ulp powers. */
+int drift_force_precision(const drift_potential *potential, int32_t precision, int64_t n,
+                          const double *xyz, double *acc, void *stream);
 
 /* Origin table of moving sources (no counterpart in the reference, whose
  * CustomOrigin tables are never built: shared/src/model.rs:193-199).

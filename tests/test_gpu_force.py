@@ -40,3 +40,39 @@ def test_device_force_matches_oracle(cuda_device, oracle, kind):
     ref = np.array([oracle.force(opot, *p) for p in xyz])
     err = np.abs(got - ref).max(axis=1) / np.abs(ref).max(axis=1)
     assert err.max() < 1e-13, (err.max(), xyz[err.argmax()])
+
+
+@pytest.mark.parametrize("kind", ["kepler", "kepler_cartesian", "plummer", "bovy"])
+def test_contraction_unit_force_is_within_a_few_ulps(cuda_device, kind):
+    """The contraction unit's force (few-ulp powers, reciprocals, rsqrt)
+    against the exact unit's correctly rounded one, over radii from 1e-3 to
+    1e3 and, for the point masses, through the out-of-line path of x^-3/2
+    (arguments outside (1e-90, 1e90))."""
+    import torch
+
+    pot = {"kepler": capi.kepler(1.0), "kepler_cartesian": capi.kepler_cartesian(1.0),
+           "plummer": capi.plummer(1.3, 0.7), "bovy": capi.bovy()}[kind]
+    rng = np.random.default_rng(11)
+    r = np.exp(rng.uniform(np.log(1e-3), np.log(1e3), 20000))
+    if kind in ("kepler", "kepler_cartesian"):
+        r = np.concatenate([r, [1e-50, 1e-47, 1e46, 1e50]])
+    u = rng.normal(size=(len(r), 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    xyz_d = torch.tensor(np.ascontiguousarray(u * r[:, None]), device="cuda")
+    exact = torch.empty_like(xyz_d)
+    fma = torch.empty_like(xyz_d)
+    capi.force_device(pot, len(r), xyz_d.data_ptr(), exact.data_ptr(), precision=capi.EXACT)
+    capi.force_device(pot, len(r), xyz_d.data_ptr(), fma.data_ptr(), precision=capi.FMA)
+    torch.cuda.synchronize()
+    e, f = exact.cpu().numpy(), fma.cpu().numpy()
+    assert np.isfinite(f).all()
+    err = np.abs(f - e).max(axis=1) / np.abs(e).max(axis=1)
+    for lo in (1e-3, 1e-2, 1e-1, 1.0, 10.0, 100.0):
+        sel = (r >= lo) & (r < 10 * lo)
+        print(f"{kind} r in [{lo:g}, {10 * lo:g}): max rel diff {err[sel].max():.2e}")
+    # Kepler and Plummer: one power and a few products, within a few ulps.
+    # Bovy: the halo's ln(1 + u) - u / (1 + u) cancels like u^2 / 2 at small
+    # radii in both units, so their one-ulp differences in each term grow
+    # there (measured: 2e-14 at r = 0.1, 8e-12 at r = 1e-3).
+    bound = 2e-15 + (4e-14 * (0.1 / r) ** 1.5 if kind == "bovy" else 0.0)
+    assert (err <= bound).all(), (err.max(), r[np.argmax(err / bound)])
