@@ -1,56 +1,37 @@
 // drift_bulge_table.h -- host construction of the bulge's incomplete-gamma
 // table (layout and evaluation in drift_potentials.cuh, bulge_lower_gamma).
 //
-// Computed in x87 extended precision (64-bit significand):
-//   series coefficients a_n = 1 / (s (s+1) ... (s+n)), n = 0..series_deg;
-//   for each centre c = first_centre + 2j the Taylor coefficients of gamma(s, .):
-//     coefficient 0 = gamma(s, c) = c^s e^-c sum_n a_n c^n (positive series),
-//     coefficient k = f^(k-1)(c) / k!  with f(x) = x^(s-1) e^-x, and by Leibniz
-//     f^(m)(x) = e^-x sum_i C(m,i) (-1)^(m-i) g_i x^(s-1-i),
-//     g_i = (s-1)(s-2)...(s-i).
+// gamma(s, x) = x^s E(x) with E(x) = int_0^1 u^(s-1) e^(-x u) du, entire.
+// Its derivatives are E^(k)(x) = (-1)^k I_k(x) with
+//   I_k(x) = int_0^1 u^(s-1+k) e^(-x u) du = gamma(s+k, x) / x^(s+k)
+//          = e^-x sum_n x^n / ((s+k) (s+k+1) ... (s+k+n)),
+// a series of positive terms (no cancellation).  Piece j holds the Taylor
+// coefficients E^(k)(c) / k!, k = 0..deg, around the centre c = 2j + 1,
+// computed in x87 extended precision (64-bit significand).
 #pragma once
 
 #include <cmath>
 
 namespace drift {
 
-inline void fill_bulge_table_impl(double s_in, double *out, int series_deg, int pieces,
-                                  int piece_deg, double first_centre)
+inline void fill_bulge_table_impl(double s_in, double *out, int pieces, int deg)
 {
     typedef long double ld;
     const ld s = s_in;
-    ld a = 1.0L / s;
-    out[0] = (double)a;
-    for (int n = 1; n <= series_deg; n++) {
-        a /= (s + n);
-        out[n] = (double)a;
-    }
-    double *piece = out + series_deg + 1;
     for (int j = 0; j < pieces; j++) {
-        const ld c = (ld)first_centre + 2.0L * j;
-        ld term = 1.0L / s, sum = term;
-        for (int n = 1; n < 2000; n++) {
-            term *= c / (s + n);
-            sum += term;
-            if (term < sum * 1e-24L) break;
-        }
+        const ld c = 2.0L * j + 1.0L;
         const ld e = expl(-c);
-        double *pc = piece + j * (piece_deg + 1);
-        pc[0] = (double)(powl(c, s) * e * sum);
         ld fact = 1.0L;
-        for (int k = 1; k <= piece_deg; k++) {
-            const int m = k - 1;
-            fact *= k;
-            ld fm = 0.0L, binom = 1.0L, g = 1.0L;
-            for (int i = 0; i <= m; i++) {
-                if (i > 0) {
-                    binom = binom * (m - i + 1) / i;
-                    g *= (s - i);
-                }
-                const ld sign = ((m - i) & 1) ? -1.0L : 1.0L;
-                fm += sign * binom * g * powl(c, s - 1.0L - i);
+        for (int k = 0; k <= deg; k++) {
+            if (k > 0) fact *= k;
+            ld term = 1.0L / (s + k), sum = term;
+            for (int n = 1; n < 4000; n++) {
+                term *= c / (s + k + n);
+                sum += term;
+                if (term < sum * 1e-22L) break;
             }
-            pc[k] = (double)(e * fm / fact);
+            const ld v = e * sum / fact;
+            out[j * (deg + 1) + k] = (double)((k & 1) ? -v : v);
         }
     }
 }

@@ -24,8 +24,7 @@
 namespace drift {
 void fill_bulge_table(double s, BulgeTable *t)
 {
-    fill_bulge_table_impl(s, t->c, BULGE_SERIES_DEG, BULGE_PIECES, BULGE_PIECE_DEG,
-                          BULGE_FIRST_CENTRE);
+    fill_bulge_table_impl(s, t->c, BULGE_PIECES, BULGE_PIECE_DEG);
 }
 }  // namespace drift
 

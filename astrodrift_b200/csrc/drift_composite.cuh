@@ -52,11 +52,9 @@ __host__ __device__ __forceinline__ double quintic(const double *c, double s)
 struct Composite {
     const drift_force_model *m;  // in the kernel's parameter space
     const double *table;         // bulge table (shared memory) for Bovy parts
-    const double *series;        // the same table in the kernel's parameter space
 
-    __device__ Composite(const drift_force_model *model, const double *bulge_table,
-                         const double *param_table = nullptr)
-        : m(model), table(bulge_table), series(param_table ? param_table : bulge_table)
+    __device__ Composite(const drift_force_model *model, const double *bulge_table)
+        : m(model), table(bulge_table)
     {
     }
 
@@ -71,7 +69,7 @@ struct Composite {
             switch (p.kind) {
             case DRIFT_POT_KEPLER: KeplerGalpy(p).force(x, y, z, fx, fy, fz); break;
             case DRIFT_POT_PLUMMER: Plummer(p).force(x, y, z, fx, fy, fz); break;
-            case DRIFT_POT_BOVY: Bovy(p, table, series).force(x, y, z, fx, fy, fz); break;
+            case DRIFT_POT_BOVY: Bovy(p, table).force(x, y, z, fx, fy, fz); break;
             case DRIFT_POT_KEPLER_CARTESIAN: KeplerCartesian(p).force(x, y, z, fx, fy, fz); break;
             default: break;
             }

@@ -130,7 +130,7 @@ struct BovyJac {
             // bulge
             {
                 double u = r2 / bulge_rc2;
-                double G = bulge_lower_gamma(table, table, bulge_s, u, bulge_gamma_s);
+                double G = bulge_lower_gamma(table, bulge_s, u, bulge_gamma_s);
                 double Gp = exp((bulge_s - 1.0) * log(u) - u) * 2.0 * r / bulge_rc2;
                 double e = Gp * xw * ir3 / r;
                 jw[0] += -bulge_k * (G * (w[0] * ir3 - x * c3) + x * e);

@@ -65,14 +65,9 @@ __device__ __forceinline__ Pot make_pot(const KernelArgs &a, const double *table
     return Pot(a.potential, table);
 }
 template <>
-__device__ __forceinline__ Bovy make_pot<Bovy>(const KernelArgs &a, const double *table)
-{
-    return Bovy(a.potential, table, a.bulge.c);
-}
-template <>
 __device__ __forceinline__ Composite make_pot<Composite>(const KernelArgs &a, const double *table)
 {
-    return Composite(&a.model, table, a.bulge.c);
+    return Composite(&a.model, table);
 }
 
 // Potentials that read the bulge table staged in shared memory.

@@ -105,50 +105,36 @@ struct Plummer {
 //
 // The host oracle follows Numerical Recipes (series / continued fraction);
 // those loops run a data-dependent number of divisions, which diverges across
-// the lanes of a warp.  The device evaluates the same function from a table
-// built on the host in extended precision:
-//   x <  6:  gamma = x^s e^-x P(x),  P(x) = sum_n x^n / (s (s+1) ... (s+n)),
-//            a positive power series truncated at degree 40 (the omitted tail
-//            is below 1e-20 of P at x = 6);
-//   6 <= x < 40: Taylor expansion of gamma(s, .) around the centres 7, 9, ..., 39,
-//            degree 18 in t = x - centre, |t| <= 1.  gamma' = x^(s-1) e^-x is
-//            singular at 0, so the expansion converges like (|t|/centre)^k:
-//            (1/7)^19 < 1e-16;
-//   x >= 40: gamma = Gamma(s) (Gamma(s, 40) < 1e-18 Gamma(s) for s <= 1.5).
-constexpr int BULGE_SERIES_DEG = 40;
-constexpr int BULGE_PIECES = 17;
-constexpr int BULGE_PIECE_DEG = 18;
-constexpr int BULGE_TABLE_SIZE = (BULGE_SERIES_DEG + 1) + BULGE_PIECES * (BULGE_PIECE_DEG + 1);
-constexpr double BULGE_X_SERIES = 6.0;
+// the lanes of a warp.  The device evaluates the same function as
+//   gamma(s, x) = x^s E(x),  E(x) = sum_n (-x)^n / (n! (s + n))  (x < 40),
+// E being entire (E(x) = int_0^1 u^(s-1) e^(-x u) du), from a table built on
+// the host in extended precision: Taylor expansions of E around the centres
+// 1, 3, ..., 39, degree 17 in t = x - centre, |t| <= 1.  Every derivative
+// obeys |E^(k)(x)| <= min(1 / (s + k), Gamma(s + k) / x^(s + k)), so the
+// omitted terms stay below 1e-16 of E over [0, 40].  Every lane runs the
+// same Horner sum and one power; for x >= 40, gamma = Gamma(s)
+// (Gamma(s, 40) < 1e-15 Gamma(s) for s <= 1.5).
+constexpr int BULGE_PIECES = 20;
+constexpr int BULGE_PIECE_DEG = 17;
+constexpr int BULGE_TABLE_SIZE = BULGE_PIECES * (BULGE_PIECE_DEG + 1);
 constexpr double BULGE_X_CONST = 40.0;
-constexpr double BULGE_FIRST_CENTRE = 7.0;
 
 struct BulgeTable {
     double c[BULGE_TABLE_SIZE];
 };
 
-// `series` and `table` hold the same coefficients: the series part is read
-// with warp-uniform indices (from the kernel parameter, where the unrolled
-// Horner loop takes them as constant operands), the Taylor pieces with
-// per-lane indices (from shared memory, where differing addresses do not
-// serialise).
-__device__ __forceinline__ double bulge_lower_gamma(const double *table, const double *series, double s,
-                                                    double x, double gamma_s)
+// `table` is the BulgeTable staged in shared memory: each lane reads its own
+// piece, and differing addresses do not serialise there.
+__device__ __forceinline__ double bulge_lower_gamma(const double *table, double s, double x, double gamma_s)
 {
-    if (x < BULGE_X_SERIES) {
-        double p = series[BULGE_SERIES_DEG];
-#pragma unroll
-        for (int n = BULGE_SERIES_DEG - 1; n >= 0; --n) p = fma(p, x, series[n]);
-        return exp(s * log(x) - x) * p;
-    }
     if (x < BULGE_X_CONST) {
-        int j = min((int)((x - (BULGE_FIRST_CENTRE - 1.0)) * 0.5), BULGE_PIECES - 1);
-        double t = x - (BULGE_FIRST_CENTRE + 2.0 * j);
-        const double *c = table + (BULGE_SERIES_DEG + 1) + j * (BULGE_PIECE_DEG + 1);
+        const int j = min((int)(x * 0.5), BULGE_PIECES - 1);
+        const double t = x - (2.0 * j + 1.0);
+        const double *c = table + j * (BULGE_PIECE_DEG + 1);
         double p = c[BULGE_PIECE_DEG];
 #pragma unroll
         for (int k = BULGE_PIECE_DEG - 1; k >= 0; --k) p = fma(p, t, c[k]);
-        return p;
+        return exp(s * log(x)) * p;
     }
     return gamma_s;
 }
@@ -159,13 +145,11 @@ struct Bovy {
     double bulge_s, bulge_rc2, bulge_k, bulge_gamma_s;
     double inv_rc2, inv_nfw_a;  // contraction unit: reciprocals formed once
     const double *table;   // BulgeTable staged in shared memory
-    const double *series;  // the same table in the kernel's parameter space
-    __device__ Bovy(const drift_potential &p, const double *bulge_table, const double *param_table = nullptr)
+    __device__ Bovy(const drift_potential &p, const double *bulge_table)
         : mn_amp(p.mn_amp), mn_a(p.mn_a), mn_b2(p.mn_b * p.mn_b), nfw_amp(p.nfw_amp),
           nfw_a(p.nfw_a), bulge_s(1.5 - 0.5 * p.bulge_alpha), bulge_rc2(p.bulge_rc * p.bulge_rc),
           bulge_k(p.bulge_k), bulge_gamma_s(p.bulge_gamma_s),
-          inv_rc2(1.0 / (p.bulge_rc * p.bulge_rc)), inv_nfw_a(1.0 / p.nfw_a), table(bulge_table),
-          series(param_table ? param_table : bulge_table)
+          inv_rc2(1.0 / (p.bulge_rc * p.bulge_rc)), inv_nfw_a(1.0 / p.nfw_a), table(bulge_table)
     {
     }
 
@@ -178,11 +162,11 @@ struct Bovy {
         if (r2s != 0.0) {
 #if DRIFT_EXACT_ARITH
             double r = sqrt(r2s);
-            double g = bulge_lower_gamma(table, series, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
+            double g = bulge_lower_gamma(table, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
             double ar_over_r = -bulge_k * g / (r2s * r);
 #else
             double inv_r = rsqrt(r2s);
-            double g = bulge_lower_gamma(table, series, bulge_s, r2s * inv_rc2, bulge_gamma_s);
+            double g = bulge_lower_gamma(table, bulge_s, r2s * inv_rc2, bulge_gamma_s);
             double ar_over_r = -bulge_k * g * (inv_r * inv_r * inv_r);
 #endif
             bx = ar_over_r * x;
