@@ -50,3 +50,22 @@ def drift_summary(pot: capi.DriftPotential, first: np.ndarray, last: np.ndarray)
     de = de[np.isfinite(de)]
     return {"median": float(np.median(de)), "p99": float(np.quantile(de, 0.99)), "max": float(de.max()),
             "particles": int(de.size)}
+
+
+def angular_momentum_drift(pot: capi.DriftPotential, first: np.ndarray, last: np.ndarray) -> dict:
+    """Median / p99 / max over particles (finite rows) of the drift of the
+    conserved angular momentum between states ``first`` and ``last`` (N, 6):
+    the full vector L = x x v for the spherical potentials (Kepler, Plummer),
+    |L(last) - L(first)| / |L(first)|; only L_z for the axisymmetric Bovy
+    potential, |L_z(last) - L_z(first)| / |L(first)| (normalised by |L| so
+    that orbits with L_z near 0 stay meaningful)."""
+    l0 = np.cross(first[:, :3], first[:, 3:])
+    l1 = np.cross(last[:, :3], last[:, 3:])
+    norm = np.linalg.norm(l0, axis=1)
+    if pot.kind == capi.POT_BOVY:
+        d, quantity = np.abs(l1[:, 2] - l0[:, 2]) / norm, "L_z"
+    else:
+        d, quantity = np.linalg.norm(l1 - l0, axis=1) / norm, "L"
+    d = d[np.isfinite(d)]
+    return {"quantity": quantity, "median": float(np.median(d)), "p99": float(np.quantile(d, 0.99)),
+            "max": float(d.max()), "particles": int(d.size)}

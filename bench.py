@@ -42,18 +42,18 @@ TS = (0.0, 100.0, 201)
 RTOL = ATOL = 1e-12
 WORKLOAD = "plummer-dop853"
 
-# Algorithmic work per unit (one accepted step of one particle), counted from
-# the integrator's arithmetic: +, -, *, /, sqrt = 1 flop; pow-type calls are
-# transcendental calls, not flops.  DOP853 stage/solution/error arithmetic is
-# 948 flops per attempt, the accept branch adds 918 (rcont, three dense
-# stages); Plummer's force is 10 flops + 1 pow per evaluation; 11 force
-# evaluations per attempt plus 4 on accept; dense output is 87 flops/sample.
-FLOPS_ATTEMPT = 948
-FLOPS_ACCEPT_EXTRA = 918
-FORCE_FLOPS = 10
-FLOPS_PER_ACCEPTED = FLOPS_ATTEMPT + FLOPS_ACCEPT_EXTRA + 15 * FORCE_FLOPS  # 2016
-FLOPS_PER_REJECTED = FLOPS_ATTEMPT + 11 * FORCE_FLOPS  # 1058
-FLOPS_PER_SAMPLE = 87
+# Algorithmic work per unit, counted exactly from the reference algorithm's
+# arithmetic (+, -, *, /, sqrt = 1 flop; pow-type calls are transcendental
+# calls, not flops): astrodrift_b200/roofline_counts.json, fitted without
+# residual over seeded runs of the restatement compiled with a counting
+# scalar.  DOP853 with the Plummer force: per accepted step, per rejected
+# step, per emitted sample and per particle (set-up).
+_COUNTS = json.loads((Path(__file__).resolve().parent / "astrodrift_b200" /
+                      "roofline_counts.json").read_text())["dop853_plummer"]["flops"]
+FLOPS_PER_ACCEPTED = _COUNTS["per_accepted"]  # 2066
+FLOPS_PER_REJECTED = _COUNTS["per_rejected"]  # 1099
+FLOPS_PER_SAMPLE = _COUNTS["per_sample"]  # 89
+FLOPS_PER_PARTICLE = _COUNTS["per_particle"]  # 128
 # DRAM bytes (read + write) per particle of one launch of this workload,
 # from the ncu capture of 262,144 particles with the ordered schedule
 # (profiles/dop853_plummer_c2.txt, section 5: 1.696 GB read + 3.397 GB
@@ -428,7 +428,7 @@ def run_config(args) -> None:
     import torch
 
     from astrodrift_b200 import capi
-    from astrodrift_b200.energy import drift_summary
+    from astrodrift_b200.energy import angular_momentum_drift, drift_summary
     from astrodrift_b200.workloads import bovy_disc, kepler_disc
 
     world, rank, local = _dist()
@@ -575,6 +575,7 @@ def run_config(args) -> None:
                                "min": int(acc_per.min())},
         "particles_not_ok": int((status != 0).sum()),
         "energy_drift": drift_summary(pot, out_first, out_last),  # rank 0's particles
+        "angular_momentum_drift": angular_momentum_drift(pot, out_first, out_last),
         "accuracy": acc_sample,
         "plain_launch": plain,
         "clocks": clocks.summary(),
@@ -822,9 +823,12 @@ def main() -> None:
     rejected = int(rej_d.cpu().numpy().astype(np.int64).sum())
     if (status != 0).any():
         raise RuntimeError(f"{int((status != 0).sum())} particles did not finish")
-    from astrodrift_b200.energy import drift_summary
+    from astrodrift_b200.energy import angular_momentum_drift, drift_summary
 
-    e_drift = drift_summary(capi.plummer(1.0, 1.0), out_d[0].cpu().numpy(), out_d[-1].cpu().numpy())
+    first_h, last_h = out_d[0].cpu().numpy(), out_d[-1].cpu().numpy()
+    e_drift = drift_summary(capi.plummer(1.0, 1.0), first_h, last_h)
+    l_drift = angular_momentum_drift(capi.plummer(1.0, 1.0), first_h, last_h)
+    del first_h, last_h
     acc_c2 = None
     if rank == 0 and not args.no_cpu:
         pick = np.sort(np.random.default_rng(777).choice(n, min(256, n), replace=False))
@@ -898,7 +902,8 @@ def main() -> None:
         hbm_peak, hbm_src = measured_hbm_gbs()
         mean_launch = statistics.mean(launch_s)
         samples = n * (nt - 1)
-        flops = accepted * FLOPS_PER_ACCEPTED + rejected * FLOPS_PER_REJECTED + samples * FLOPS_PER_SAMPLE
+        flops = (accepted * FLOPS_PER_ACCEPTED + rejected * FLOPS_PER_REJECTED + samples * FLOPS_PER_SAMPLE
+                 + n * FLOPS_PER_PARTICLE)
         achieved_tflops = flops / mean_launch / 1e12
         bytes_alg = 48 * n * (nt + 1) + 8 * nt + 12 * n
         cpu = None
@@ -944,12 +949,15 @@ def main() -> None:
                          "flops_per_launch": flops,
                          "units": f"{accepted} accepted x {FLOPS_PER_ACCEPTED} + {rejected} "
                                   f"rejected x {FLOPS_PER_REJECTED} + {samples} samples x "
-                                  f"{FLOPS_PER_SAMPLE}"},
+                                  f"{FLOPS_PER_SAMPLE} + {n} particles x {FLOPS_PER_PARTICLE}",
+                         "counts_source": "astrodrift_b200/roofline_counts.json (exact operation counts "
+                                          "of the reference algorithm)"},
             "roofline_hbm": {"bound": "hbm", "achieved": bytes_alg / mean_launch / 1e9,
                              "peak": hbm_peak, "unit": "GB/s",
                              "frac": bytes_alg / mean_launch / 1e9 / hbm_peak, "peak_source": hbm_src},
             "kernel_ms_mean": 1e3 * mean_launch,
             "energy_drift": e_drift,
+            "angular_momentum_drift": l_drift,
             "accuracy": acc_c2,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "accepted steps/s",

@@ -1,0 +1,27 @@
+"""The committed operation counts (astrodrift_b200/roofline_counts.json, which
+the benchmark's roofline divides by) are reproduced by counting the oracle's
+arithmetic again, and the per-unit model fits every run exactly."""
+
+from __future__ import annotations
+
+import json
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_committed_counts_match_a_fresh_count():
+    sys.path.insert(0, str(ROOT / "oracle"))
+    try:
+        import roofline_counts
+    finally:
+        sys.path.pop(0)
+    rows = roofline_counts.run_counts()
+    committed = json.loads((ROOT / "astrodrift_b200" / "roofline_counts.json").read_text())
+    for name, r in rows.items():
+        assert roofline_counts.fit(r) == committed[name], name  # fit() raises unless exact
+    plummer = committed["dop853_plummer"]["flops"]
+    # the survey's hand count for DOP853 + Plummer was about 2,065 per accepted step
+    assert abs(plummer["per_accepted"] - 2065) < 50
+    assert committed["dop853_plummer"]["pow"]["per_accepted"] == 17  # 15 forces + 2 controller pows
