@@ -21,6 +21,8 @@
 // component instead.
 #pragma once
 
+#include <type_traits>
+
 #include "drift_common.cuh"
 #include "drift_composite.cuh"
 
@@ -196,6 +198,14 @@ constexpr double FACC2 = 1.0 / 6.0;
 // step h = 1e3 * UROUND forever in that situation.
 constexpr int DOP853_NONFINITE_LIMIT = 64;
 
+
+// Potentials whose force is large enough that the accept branch evaluates
+// its three extra stages from one call site instead of three inlined copies.
+template <class Pot>
+__host__ __device__ constexpr bool compact_extra_stages()
+{
+    return std::is_same<Pot, Bovy>::value || std::is_same<Pot, Composite>::value;
+}
 
 template <class Pot>
 struct Dop853Lane {
@@ -410,24 +420,67 @@ struct Dop853Lane {
                     D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
                     D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
             }
+            if constexpr (compact_extra_stages<Pot>()) {
+                // Stages 14..16 around one force call site: for the heavy
+                // forces the step body, inlined once per force evaluation,
+                // otherwise overflows the instruction cache.
+#pragma unroll 1
+                for (int e = 14; e <= 16; e++) {
+                    double tq;
+                    if (e == 14) {
 #pragma unroll
-            for (int i = 0; i < 6; i++)
-                yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] + A149 * k9[i] +
-                                     A1410 * k10[i] + A1411 * k2[i] + A1412 * k3[i] +
-                                     A1413 * k4[i]);
-            rhs(pot, t_old + C14 * h, yy1, k10);
+                        for (int i = 0; i < 6; i++)
+                            yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] +
+                                                 A149 * k9[i] + A1410 * k10[i] + A1411 * k2[i] +
+                                                 A1412 * k3[i] + A1413 * k4[i]);
+                        tq = t_old + C14 * h;
+                    } else if (e == 15) {
 #pragma unroll
-            for (int i = 0; i < 6; i++)
-                yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] + A158 * k8[i] +
-                                     A1511 * k2[i] + A1512 * k3[i] + A1513 * k4[i] +
-                                     A1514 * k10[i]);
-            rhs(pot, t_old + C15 * h, yy1, k2);
+                        for (int i = 0; i < 6; i++)
+                            yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] +
+                                                 A158 * k8[i] + A1511 * k2[i] + A1512 * k3[i] +
+                                                 A1513 * k4[i] + A1514 * k10[i]);
+                        tq = t_old + C15 * h;
+                    } else {
 #pragma unroll
-            for (int i = 0; i < 6; i++)
-                yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] + A168 * k8[i] +
-                                     A169 * k9[i] + A1613 * k4[i] + A1614 * k10[i] +
-                                     A1615 * k2[i]);
-            rhs(pot, t_old + C16 * h, yy1, k3);
+                        for (int i = 0; i < 6; i++)
+                            yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] +
+                                                 A168 * k8[i] + A169 * k9[i] + A1613 * k4[i] +
+                                                 A1614 * k10[i] + A1615 * k2[i]);
+                        tq = t_old + C16 * h;
+                    }
+                    double f[6];
+                    rhs(pot, tq, yy1, f);
+#pragma unroll
+                    for (int i = 0; i < 6; i++) {
+                        if (e == 14)
+                            k10[i] = f[i];
+                        else if (e == 15)
+                            k2[i] = f[i];
+                        else
+                            k3[i] = f[i];
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+                    yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] + A149 * k9[i] +
+                                         A1410 * k10[i] + A1411 * k2[i] + A1412 * k3[i] +
+                                         A1413 * k4[i]);
+                rhs(pot, t_old + C14 * h, yy1, k10);
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+                    yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] + A158 * k8[i] +
+                                         A1511 * k2[i] + A1512 * k3[i] + A1513 * k4[i] +
+                                         A1514 * k10[i]);
+                rhs(pot, t_old + C15 * h, yy1, k2);
+#pragma unroll
+                for (int i = 0; i < 6; i++)
+                    yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] + A168 * k8[i] +
+                                         A169 * k9[i] + A1613 * k4[i] + A1614 * k10[i] +
+                                         A1615 * k2[i]);
+                rhs(pot, t_old + C16 * h, yy1, k3);
+            }
 
             // rcont1..4 (dop853.rs:636-642) need only y, y_new, k1 and k4,
             // so they are formed here, after the extra stages.
