@@ -185,6 +185,90 @@ __device__ __forceinline__ double pow_1p5_few_ulp(double x)
 
 __device__ __forceinline__ double root8_few_ulp(double x) { return sqrt(sqrt(sqrt(x))); }
 
+// Natural log and exp for the contraction unit, from their series (no
+// vendor code): each call site inlines about half the instructions of the
+// library functions, which matters where a force is inlined at every stage.
+//   log x = k ln2 + 2 atanh(t),  x = 2^k m with m in [sqrt(1/2), sqrt(2)),
+//           t = (m - 1) / (m + 1), |t| <= 0.1716, atanh t = sum_j t^(2j+1) / (2j+1);
+//           terms to j = 10 leave less than 2^-55 of the sum.
+//   exp x = 2^k e^r,  k = rint(x / ln2), r = x - k ln2 with ln2 in two parts,
+//           |r| <= 0.3466, e^r = sum_{n <= 13} r^n / n! (remainder < 2^-56 of e^r).
+// Within a few ulps for normal positive x (log) and |x| < 708 (exp); every
+// other argument takes the library function out of line.
+constexpr double LN2_HI = 0.6931471805599453;
+constexpr double LN2_LO = 2.3190468138462996e-17;
+constexpr double LOG2_E = 1.4426950408889634;
+
+static __device__ __noinline__ double log_rare(double x) { return log(x); }
+static __device__ __noinline__ double exp_rare(double x) { return exp(x); }
+
+__device__ __forceinline__ double log_few_ulp(double x)
+{
+    if (!(x >= 2.2250738585072014e-308 && x <= 1.7976931348623157e308)) return log_rare(x);
+    const long long bits = __double_as_longlong(x);
+    int k = (int)(bits >> 52) - 1023;
+    double m = __longlong_as_double((bits & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);  // [1, 2)
+    if (m > 1.4142135623730951) {
+        m *= 0.5;
+        k += 1;
+    }
+    const double t = (m - 1.0) * fast_rcp(m + 1.0);
+    const double z = t * t;
+    double p = 1.0 / 21.0;
+    p = fma(p, z, 1.0 / 19.0);
+    p = fma(p, z, 1.0 / 17.0);
+    p = fma(p, z, 1.0 / 15.0);
+    p = fma(p, z, 1.0 / 13.0);
+    p = fma(p, z, 1.0 / 11.0);
+    p = fma(p, z, 1.0 / 9.0);
+    p = fma(p, z, 1.0 / 7.0);
+    p = fma(p, z, 1.0 / 5.0);
+    p = fma(p, z, 1.0 / 3.0);
+    const double lm = 2.0 * fma(t * z, p, t);  // 2 (t + t^3 p)
+    const double kd = (double)k;
+    return fma(kd, LN2_HI, fma(kd, LN2_LO, lm));
+}
+
+__device__ __forceinline__ double exp_few_ulp(double x)
+{
+    if (!(fabs(x) < 708.0)) return exp_rare(x);
+    const double kd = rint(x * LOG2_E);
+    const double r = fma(-kd, LN2_LO, fma(-kd, LN2_HI, x));
+    double p = 1.0 / 6227020800.0;          // 1/13!
+    p = fma(p, r, 1.0 / 479001600.0);       // 1/12!
+    p = fma(p, r, 1.0 / 39916800.0);
+    p = fma(p, r, 1.0 / 3628800.0);
+    p = fma(p, r, 1.0 / 362880.0);
+    p = fma(p, r, 1.0 / 40320.0);
+    p = fma(p, r, 1.0 / 5040.0);
+    p = fma(p, r, 1.0 / 720.0);
+    p = fma(p, r, 1.0 / 120.0);
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    return p * __longlong_as_double((long long)((int)kd + 1023) << 52);
+}
+
+__device__ __forceinline__ double unit_log(double x)
+{
+#if DRIFT_EXACT_ARITH
+    return log(x);
+#else
+    return log_few_ulp(x);
+#endif
+}
+
+__device__ __forceinline__ double unit_exp(double x)
+{
+#if DRIFT_EXACT_ARITH
+    return exp(x);
+#else
+    return exp_few_ulp(x);
+#endif
+}
+
 // log2(q) for the DOPR54 controller, whose result is only rounded to an
 // integer after scaling by 0.1: in the contraction unit the exponent plus a
 // single-precision log2 of the mantissa in [1, 2) (absolute error ~1e-7,

@@ -134,7 +134,7 @@ __device__ __forceinline__ double bulge_lower_gamma(const double *table, double 
         double p = c[BULGE_PIECE_DEG];
 #pragma unroll
         for (int k = BULGE_PIECE_DEG - 1; k >= 0; --k) p = fma(p, t, c[k]);
-        return exp(s * log(x)) * p;
+        return unit_exp(s * unit_log(x)) * p;
     }
     return gamma_s;
 }
@@ -212,7 +212,7 @@ struct Bovy {
             double inv_r = rsqrt(r2);
             double r = r2 * inv_r;
             double u = r * inv_nfw_a;
-            double term = log(1. + u) - u * fast_rcp(1.0 + u);
+            double term = unit_log(1. + u) - u * fast_rcp(1.0 + u);
             double ar_over_r = -nfw_amp * term * (inv_r * inv_r * inv_r);
             hx = ar_over_r * x;
             hy = ar_over_r * y;
