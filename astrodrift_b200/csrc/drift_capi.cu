@@ -276,6 +276,7 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.tape_steps = L->tape_steps;
     a.arbitrary_times = L->arbitrary_times != 0;
     a.tape_stride = L->tape_stride;
+    a.sparse_output = L->nt <= drift::SPARSE_OUTPUT_NT;
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
@@ -405,6 +406,7 @@ int launch_batch(int sm_count, const drift_launch *R, int32_t count, void *ws, c
         S.n_accepted = R[i].n_accepted;
         S.n_rejected = R[i].n_rejected;
         first += R[i].n;
+        if (R[i].nt > drift::SPARSE_OUTPUT_NT) a.sparse_output = 0;
     }
     a.n = first;
     geometry.n = first;

@@ -283,7 +283,8 @@ struct Dop853Lane {
     template <bool TAPE = false, class Out>
     __device__ __forceinline__ bool step(const Pot &pot, const Grid &grid, double rtol,
                                          double atol, Out &out, volatile double *park,
-                                         double *tape_row = nullptr, double *h_slot = nullptr)
+                                         double *tape_row = nullptr, double *h_slot = nullptr,
+                                         bool sparse_output = false)
     {
         using namespace dop853c;
         const int RCONT_STRIDE = blockDim.x;
@@ -405,131 +406,143 @@ struct Dop853Lane {
             }
             rhs(pot, t_new, k5, k4);  // FSAL: k4 = f(t_new, y_new)
 
-#pragma unroll
-            for (int i = 0; i < 6; i++) {
-                park[(0 * 6 + i) * RCONT_STRIDE] =
-                    D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
-                    D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
-                park[(1 * 6 + i) * RCONT_STRIDE] =
-                    D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
-                    D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
-                park[(2 * 6 + i) * RCONT_STRIDE] =
-                    D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
-                    D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
-                park[(3 * 6 + i) * RCONT_STRIDE] =
-                    D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
-                    D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
-            }
-            if constexpr (compact_extra_stages<Pot>()) {
-                // Stages 14..16 around one force call site: for the heavy
-                // forces the step body, inlined once per force evaluation,
-                // otherwise overflows the instruction cache.
-#pragma unroll 1
-                for (int e = 14; e <= 16; e++) {
-                    double tq;
-                    if (e == 14) {
-#pragma unroll
-                        for (int i = 0; i < 6; i++)
-                            yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] +
-                                                 A149 * k9[i] + A1410 * k10[i] + A1411 * k2[i] +
-                                                 A1412 * k3[i] + A1413 * k4[i]);
-                        tq = t_old + C14 * h;
-                    } else if (e == 15) {
-#pragma unroll
-                        for (int i = 0; i < 6; i++)
-                            yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] +
-                                                 A158 * k8[i] + A1511 * k2[i] + A1512 * k3[i] +
-                                                 A1513 * k4[i] + A1514 * k10[i]);
-                        tq = t_old + C15 * h;
-                    } else {
-#pragma unroll
-                        for (int i = 0; i < 6; i++)
-                            yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] +
-                                                 A168 * k8[i] + A169 * k9[i] + A1613 * k4[i] +
-                                                 A1614 * k10[i] + A1615 * k2[i]);
-                        tq = t_old + C16 * h;
-                    }
-                    double f[6];
-                    rhs(pot, tq, yy1, f);
-#pragma unroll
-                    for (int i = 0; i < 6; i++) {
-                        if (e == 14)
-                            k10[i] = f[i];
-                        else if (e == 15)
-                            k2[i] = f[i];
-                        else
-                            k3[i] = f[i];
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int i = 0; i < 6; i++)
-                    yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] + A149 * k9[i] +
-                                         A1410 * k10[i] + A1411 * k2[i] + A1412 * k3[i] +
-                                         A1413 * k4[i]);
-                rhs(pot, t_old + C14 * h, yy1, k10);
-#pragma unroll
-                for (int i = 0; i < 6; i++)
-                    yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] + A158 * k8[i] +
-                                         A1511 * k2[i] + A1512 * k3[i] + A1513 * k4[i] +
-                                         A1514 * k10[i]);
-                rhs(pot, t_old + C15 * h, yy1, k2);
-#pragma unroll
-                for (int i = 0; i < 6; i++)
-                    yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] + A168 * k8[i] +
-                                         A169 * k9[i] + A1613 * k4[i] + A1614 * k10[i] +
-                                         A1615 * k2[i]);
-                rhs(pot, t_old + C16 * h, yy1, k3);
-            }
+            // The three extra stages and rcont1..8 serve only the dense output
+            // of this step.  On sparse grids (a launch-uniform flag) a lane
+            // with no requested time in (t_old, t_new) skips them; emitted
+            // samples are unchanged.
+            const bool skip_dense =
+                sparse_output && !(next < grid.nt - 1 && pos_neg * grid.at(next + 1) < pos_neg * t_new);
+            if (!skip_dense) {
 
-            // rcont1..4 (dop853.rs:636-642) need only y, y_new, k1 and k4,
-            // so they are formed here, after the extra stages.
-            double r1[6], r2[6], r3[6], r4[6], r5[6], r6[6], r7[6], r8[6];
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    park[(0 * 6 + i) * RCONT_STRIDE] =
+                        D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
+                        D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
+                    park[(1 * 6 + i) * RCONT_STRIDE] =
+                        D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
+                        D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
+                    park[(2 * 6 + i) * RCONT_STRIDE] =
+                        D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
+                        D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
+                    park[(3 * 6 + i) * RCONT_STRIDE] =
+                        D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
+                        D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
+                }
+                if constexpr (compact_extra_stages<Pot>()) {
+                    // Stages 14..16 around one force call site: for the heavy
+                    // forces the step body, inlined once per force evaluation,
+                    // otherwise overflows the instruction cache.
+#pragma unroll 1
+                    for (int e = 14; e <= 16; e++) {
+                        double tq;
+                        if (e == 14) {
+#pragma unroll
+                            for (int i = 0; i < 6; i++)
+                                yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] +
+                                                     A149 * k9[i] + A1410 * k10[i] + A1411 * k2[i] +
+                                                     A1412 * k3[i] + A1413 * k4[i]);
+                            tq = t_old + C14 * h;
+                        } else if (e == 15) {
+#pragma unroll
+                            for (int i = 0; i < 6; i++)
+                                yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] +
+                                                     A158 * k8[i] + A1511 * k2[i] + A1512 * k3[i] +
+                                                     A1513 * k4[i] + A1514 * k10[i]);
+                            tq = t_old + C15 * h;
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 6; i++)
+                                yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] +
+                                                     A168 * k8[i] + A169 * k9[i] + A1613 * k4[i] +
+                                                     A1614 * k10[i] + A1615 * k2[i]);
+                            tq = t_old + C16 * h;
+                        }
+                        double f[6];
+                        rhs(pot, tq, yy1, f);
+#pragma unroll
+                        for (int i = 0; i < 6; i++) {
+                            if (e == 14)
+                                k10[i] = f[i];
+                            else if (e == 15)
+                                k2[i] = f[i];
+                            else
+                                k3[i] = f[i];
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 6; i++)
+                        yy1[i] = y[i] + h * (A141 * k1[i] + A147 * k7[i] + A148 * k8[i] + A149 * k9[i] +
+                                             A1410 * k10[i] + A1411 * k2[i] + A1412 * k3[i] +
+                                             A1413 * k4[i]);
+                    rhs(pot, t_old + C14 * h, yy1, k10);
+#pragma unroll
+                    for (int i = 0; i < 6; i++)
+                        yy1[i] = y[i] + h * (A151 * k1[i] + A156 * k6[i] + A157 * k7[i] + A158 * k8[i] +
+                                             A1511 * k2[i] + A1512 * k3[i] + A1513 * k4[i] +
+                                             A1514 * k10[i]);
+                    rhs(pot, t_old + C15 * h, yy1, k2);
+#pragma unroll
+                    for (int i = 0; i < 6; i++)
+                        yy1[i] = y[i] + h * (A161 * k1[i] + A166 * k6[i] + A167 * k7[i] + A168 * k8[i] +
+                                             A169 * k9[i] + A1613 * k4[i] + A1614 * k10[i] +
+                                             A1615 * k2[i]);
+                    rhs(pot, t_old + C16 * h, yy1, k3);
+                }
+
+                // rcont1..4 (dop853.rs:636-642) need only y, y_new, k1 and k4,
+                // so they are formed here, after the extra stages.
+                double r1[6], r2[6], r3[6], r4[6], r5[6], r6[6], r7[6], r8[6];
+#pragma unroll
+                for (int i = 0; i < 6; i++) {
+                    r5[i] = h * (park[(0 * 6 + i) * RCONT_STRIDE] + D413 * k4[i] + D414 * k10[i] +
+                                 D415 * k2[i] + D416 * k3[i]);
+                    r6[i] = h * (park[(1 * 6 + i) * RCONT_STRIDE] + D513 * k4[i] + D514 * k10[i] +
+                                 D515 * k2[i] + D516 * k3[i]);
+                    r7[i] = h * (park[(2 * 6 + i) * RCONT_STRIDE] + D613 * k4[i] + D614 * k10[i] +
+                                 D615 * k2[i] + D616 * k3[i]);
+                    r8[i] = h * (park[(3 * 6 + i) * RCONT_STRIDE] + D713 * k4[i] + D714 * k10[i] +
+                                 D715 * k2[i] + D716 * k3[i]);
+                    r1[i] = y[i];
+                    double ydiff = k5[i] - y[i];
+                    r2[i] = ydiff;
+                    double bspl = h * k1[i] - ydiff;
+                    r3[i] = bspl;
+                    r4[i] = ydiff - h * k4[i] - bspl;
+                }
+
+                // Dense output of every requested time strictly before t_current.
+#if !DRIFT_EXACT_ARITH
+                const double inv_h = fast_rcp(h);
+#endif
+                while (next < grid.nt - 1) {
+                    double tk = grid.at(next + 1);
+                    if (!(pos_neg * tk < pos_neg * t_new)) break;
+#if DRIFT_EXACT_ARITH
+                    double s = (tk - t_old) / h;
+#else
+                    double s = (tk - t_old) * inv_h;
+#endif
+                    double s1 = 1.0 - s;
+                    double yy[6];
+#pragma unroll
+                    for (int i = 0; i < 6; i++)
+                        yy[i] = r1[i] +
+                                s * (r2[i] +
+                                     s1 * (r3[i] +
+                                           s * (r4[i] +
+                                                s1 * (r5[i] + s * (r6[i] + s1 * (r7[i] + s * r8[i]))))));
+                    out.write(next + 1, yy);
+                    next += 1;
+                }
+            }
 #pragma unroll
             for (int i = 0; i < 6; i++) {
-                r5[i] = h * (park[(0 * 6 + i) * RCONT_STRIDE] + D413 * k4[i] + D414 * k10[i] +
-                             D415 * k2[i] + D416 * k3[i]);
-                r6[i] = h * (park[(1 * 6 + i) * RCONT_STRIDE] + D513 * k4[i] + D514 * k10[i] +
-                             D515 * k2[i] + D516 * k3[i]);
-                r7[i] = h * (park[(2 * 6 + i) * RCONT_STRIDE] + D613 * k4[i] + D614 * k10[i] +
-                             D615 * k2[i] + D616 * k3[i]);
-                r8[i] = h * (park[(3 * 6 + i) * RCONT_STRIDE] + D713 * k4[i] + D714 * k10[i] +
-                             D715 * k2[i] + D716 * k3[i]);
-                r1[i] = y[i];
-                double ydiff = k5[i] - y[i];
-                r2[i] = ydiff;
-                double bspl = h * k1[i] - ydiff;
-                r3[i] = bspl;
-                r4[i] = ydiff - h * k4[i] - bspl;
                 k1[i] = k4[i];
                 y[i] = k5[i];
             }
             t_cur = t_new;
-
-            // Dense output of every requested time strictly before t_current.
-#if !DRIFT_EXACT_ARITH
-            const double inv_h = fast_rcp(h);
-#endif
-            while (next < grid.nt - 1) {
-                double tk = grid.at(next + 1);
-                if (!(pos_neg * tk < pos_neg * t_cur)) break;
-#if DRIFT_EXACT_ARITH
-                double s = (tk - t_old) / h;
-#else
-                double s = (tk - t_old) * inv_h;
-#endif
-                double s1 = 1.0 - s;
-                double yy[6];
-#pragma unroll
-                for (int i = 0; i < 6; i++)
-                    yy[i] = r1[i] +
-                            s * (r2[i] +
-                                 s1 * (r3[i] +
-                                       s * (r4[i] +
-                                            s1 * (r5[i] + s * (r6[i] + s1 * (r7[i] + s * r8[i]))))));
-                out.write(next + 1, yy);
-                next += 1;
-            }
             done = (next >= grid.nt - 1);
 
             hnew = fabs(hnew) > fabs(hmax) ? pos_neg * hmax : hnew;

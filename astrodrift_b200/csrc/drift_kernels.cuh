@@ -262,9 +262,10 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
                     row = (nacc % m == 0) ? block + (nacc / m) * 8 : nullptr;
                     h_slot = block + ncp * 8 + nacc;
                 }
-                accepted = l853.template step<true>(pot, grid, a.rtol, a.atol, out, park, row, h_slot);
+                accepted = l853.template step<true>(pot, grid, a.rtol, a.atol, out, park, row, h_slot,
+                                                    a.sparse_output != 0);
             } else {
-                accepted = l853.step(pot, grid, a.rtol, a.atol, out, park);
+                accepted = l853.step(pot, grid, a.rtol, a.atol, out, park, nullptr, nullptr, a.sparse_output != 0);
             }
             if (!accepted && l853.nonfinite_run >= DOP853_NONFINITE_LIMIT) {
                 nrej++;

@@ -34,6 +34,12 @@ struct Segment {
     uint32_t *n_rejected;
 };
 
+// Grids with at most this many output times count as sparse: DOP853 then
+// skips the dense-output stages of steps that emit no sample.  (With dense
+// grids most warps emit somewhere in most steps, and warps that take and
+// skip the block at different times thrash the instruction cache.)
+constexpr int SPARSE_OUTPUT_NT = 8;
+
 // Everything a launch needs, passed by value as the kernel parameter.
 struct KernelArgs {
     int64_t n;
@@ -61,6 +67,7 @@ struct KernelArgs {
     int32_t nsegs;               // batched launch: requests in segs[], 0 = single request
     int32_t arbitrary_times;     // DOPR54: intervals end at ts[i + 1]
     int32_t tape_stride;         // step tape layout (see drift_launch.tape_stride)
+    int32_t sparse_output;       // every grid has <= SPARSE_OUTPUT_NT times (see Dop853Lane::step)
     drift_potential potential;
     BulgeTable bulge;            // Bovy (or a force model with Bovy parts): incomplete gamma table
     drift_force_model model;     // potential.kind == DRIFT_POT_MODEL: the summed force

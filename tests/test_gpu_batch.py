@@ -110,3 +110,38 @@ def test_ordered_batch_rejects_a_workspace_for_one_request(cuda_device):
     rc = capi.lib().drift_integrate_batch(arr, 3, ctypes.c_void_p(0))
     assert rc == 3  # DRIFT_ERROR_WORKSPACE
     assert "workspace" in capi.lib().drift_last_error().decode()
+
+
+@pytest.mark.parametrize("precision", [capi.EXACT, capi.FMA])
+def test_sparse_output_skip_leaves_results_unchanged(cuda_device, precision):
+    """A grid of at most 8 output times lets DOP853 skip the dense-output
+    stages of steps that emit nothing; alone, such a request runs that way,
+    batched with a dense request it does not.  Both runs must agree bit for
+    bit (Bovy force: the step with the looped extra stages)."""
+    import torch
+
+    dev = torch.device("cuda:0")
+    rng = np.random.default_rng(8)
+    pot = capi.bovy()
+    reqs = _requests(rng, count=2)
+    reqs[0]["ts"] = np.linspace(0.0, 30.0, 3)           # sparse
+    reqs[1] = dict(y0=reqs[1]["y0"], ts=np.linspace(0.0, 20.0, 40))  # dense
+    outs = []
+    for batched in (False, True):
+        launches, keeps = [], []
+        for req in (reqs if batched else reqs[:1]):
+            L, keep = _launch(torch, capi.DOP853, pot, req, capi.PERSISTENT, dev)
+            L.precision = precision
+            launches.append(L)
+            keeps.append(keep)
+        total = sum(len(r["y0"]) for r in reqs)
+        probe = capi.make_launch(capi.DOP853, pot, total, 2, rtol=1e-10, atol=1e-10,
+                                 schedule=capi.PERSISTENT)
+        ws = torch.zeros(max(capi.query_workspace(probe), 8), dtype=torch.uint8, device=dev)
+        launches[0].workspace, launches[0].workspace_bytes = ws.data_ptr(), ws.numel()
+        capi.integrate_batch_device(launches, torch.cuda.current_stream().cuda_stream)
+        torch.cuda.synchronize()
+        outs.append([t.cpu().numpy() for t in keeps[0][2:]])
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
+    assert np.isfinite(outs[0][0]).all()
