@@ -788,8 +788,12 @@ int drift_integrate_host(const drift_launch *L)
         DRIFT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         const size_t budget = std::min<size_t>(free_b / 4, size_t(8) << 30);
         int64_t by_mem = (int64_t)(budget / (nt * row));
-        // at least two chunks when the output is large so copies overlap compute
-        int64_t target = n > 65536 ? (n + 3) / 4 : n;
+        // Several chunks when the output is large, so the device->host copy
+        // of one chunk overlaps the integration of the next; the copy of the
+        // whole output usually takes longer than its integration, and only
+        // the first chunk's integration is not hidden behind a copy.
+        const int64_t parts = n > 524288 ? 8 : (n > 65536 ? 4 : 1);
+        int64_t target = (n + parts - 1) / parts;
         chunk = std::max<int64_t>(1, std::min(target, by_mem));
         if (chunk < n) chunk = std::max<int64_t>(128, chunk / 128 * 128);
         chunk = std::min(chunk, n);
