@@ -792,7 +792,7 @@ int drift_integrate_host(const drift_launch *L)
         // of one chunk overlaps the integration of the next; the copy of the
         // whole output usually takes longer than its integration, and only
         // the first chunk's integration is not hidden behind a copy.
-        const int64_t parts = n > 524288 ? 8 : (n > 65536 ? 4 : 1);
+        const int64_t parts = n > 524288 ? 16 : (n > 65536 ? 4 : 1);
         int64_t target = (n + parts - 1) / parts;
         chunk = std::max<int64_t>(1, std::min(target, by_mem));
         if (chunk < n) chunk = std::max<int64_t>(128, chunk / 128 * 128);
