@@ -46,6 +46,10 @@ EXPORTED = (
     "drift_query_workspace",
     "drift_integrate",
     "drift_integrate_host",
+    "drift_context_create",
+    "drift_context_integrate_host",
+    "drift_context_memory",
+    "drift_context_destroy",
     "drift_galpy_dopr54",
     "drift_galpy_dop853",
     "drift_force",
@@ -199,6 +203,11 @@ def lib() -> ctypes.CDLL:
         L.drift_query_workspace.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.POINTER(ctypes.c_size_t)]
         L.drift_integrate.argtypes = [ctypes.POINTER(DriftLaunch), ctypes.c_void_p]
         L.drift_integrate_host.argtypes = [ctypes.POINTER(DriftLaunch)]
+        L.drift_context_create.argtypes = [ctypes.c_int32, ctypes.POINTER(ctypes.c_void_p)]
+        L.drift_context_integrate_host.argtypes = [ctypes.c_void_p, ctypes.POINTER(DriftLaunch)]
+        L.drift_context_memory.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_size_t),
+                                           ctypes.POINTER(ctypes.c_size_t)]
+        L.drift_context_destroy.argtypes = [ctypes.c_void_p]
         L.drift_galpy_dopr54.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 3 + [ctypes.c_void_p]
         L.drift_galpy_dop853.argtypes = [ctypes.c_void_p] * 3 + [ctypes.c_int64] * 2 + [ctypes.c_double] * 2 + [ctypes.c_void_p]
         L.drift_force.argtypes = [ctypes.POINTER(DriftPotential), ctypes.c_int64, ctypes.c_void_p,
@@ -322,10 +331,13 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
                    precision: int = EXACT, schedule: int = PERSISTENT, block_size: int = 0,
                    dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
                    timeout_s: float = 0.0, want_out: bool = True, out=None,
-                   model: DriftForceModel | None = None, arbitrary_times: bool = False) -> dict:
+                   model: DriftForceModel | None = None, arbitrary_times: bool = False,
+                   context: "Context | None" = None) -> dict:
     """drift_integrate_host: host arrays in, host arrays out.  With `model`
     (whose origin table is a host array), `pot` is ignored and the stage
-    integrates in the summed force."""
+    integrates in the summed force.  With `context`, the call runs on that
+    explicit context (drift_context_integrate_host) instead of the device's
+    implicit one."""
     y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
     n = y0.shape[0]
     if ts is not None:
@@ -360,8 +372,55 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
     L.err_code = _ptr(res["err"])
     L.n_accepted = _ptr(res["accepted"])
     L.n_rejected = _ptr(res["rejected"])
-    check(lib().drift_integrate_host(ctypes.byref(L)), "drift_integrate_host")
+    if context is not None:
+        check(lib().drift_context_integrate_host(context.handle(), ctypes.byref(L)),
+              "drift_context_integrate_host")
+    else:
+        check(lib().drift_integrate_host(ctypes.byref(L)), "drift_integrate_host")
     return res
+
+
+class Context:
+    """An explicit host-path context (drift_context_*): its own streams and
+    grow-only buffers on one device, freed by close().
+
+        with capi.Context(device=0) as ctx:
+            res = capi.integrate_host(capi.DOP853, pot, y0, ts=ts, context=ctx)
+            ctx.memory()       # (device bytes, page-locked host bytes) held
+    """
+
+    def __init__(self, device: int | None = None):
+        self._ptr = ctypes.c_void_p()
+        check(lib().drift_context_create(-1 if device is None else int(device), ctypes.byref(self._ptr)),
+              "drift_context_create")
+
+    def handle(self) -> ctypes.c_void_p:
+        if not self._ptr:
+            raise RuntimeError("the context is closed")
+        return self._ptr
+
+    def memory(self) -> tuple[int, int]:
+        dev, pinned = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        check(lib().drift_context_memory(self.handle(), ctypes.byref(dev), ctypes.byref(pinned)),
+              "drift_context_memory")
+        return dev.value, pinned.value
+
+    def close(self) -> None:
+        if self._ptr:
+            lib().drift_context_destroy(self._ptr)
+            self._ptr = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def query_workspace(L: DriftLaunch) -> int:

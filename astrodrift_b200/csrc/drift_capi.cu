@@ -68,6 +68,12 @@ struct DevBuf {
         if (e == cudaSuccess) bytes = need;
         return e;
     }
+    void release()
+    {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
     template <class T>
     T *as() const
     {
@@ -88,10 +94,18 @@ struct HostBuf {
         if (e == cudaSuccess) bytes = need;
         return e;
     }
+    void release()
+    {
+        if (ptr) cudaFreeHost(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
 };
 
-// Library-owned state of one device: created on first use, kept for the
-// life of the process.
+// State of the host path on one device: two streams and grow-only device
+// and page-locked buffers.  The implicit context of each device is created
+// on first use and kept for the life of the process; explicit ones
+// (drift_context_create) are freed by drift_context_destroy.
 struct DeviceContext {
     int device = -1;
     int sm_count = 0;
@@ -101,6 +115,33 @@ struct DeviceContext {
     DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor, origins;
     DevBuf src_traj, src_table, src_origins;  // drift_origin_table_host
     HostBuf stage[2];
+
+    DevBuf *dev_bufs[14] = {&y0, &grid, &out[0], &out[1], &yfin, &status, &err, &acc, &rej, &cursor,
+                            &origins, &src_traj, &src_table, &src_origins};
+
+    // Streams and events on `device` (which must be current).
+    int init(int dev);
+    size_t device_bytes() const
+    {
+        size_t b = 0;
+        for (const DevBuf *d : dev_bufs) b += d->bytes;
+        return b;
+    }
+    size_t pinned_bytes() const { return stage[0].bytes + stage[1].bytes; }
+    // Waits for the streams and frees every buffer, stream and event (device current).
+    void release()
+    {
+        for (int i = 0; i < 2; i++)
+            if (streams[i]) cudaStreamSynchronize(streams[i]);
+        for (DevBuf *d : dev_bufs) d->release();
+        for (int i = 0; i < 2; i++) {
+            stage[i].release();
+            if (done[i]) cudaEventDestroy(done[i]);
+            if (streams[i]) cudaStreamDestroy(streams[i]);
+            done[i] = nullptr;
+            streams[i] = nullptr;
+        }
+    }
 };
 
 std::mutex g_ctx_mu;
@@ -115,20 +156,44 @@ int current_context(DeviceContext **out)
     if ((int)g_ctx.size() <= dev) g_ctx.resize(dev + 1, nullptr);
     if (!g_ctx[dev]) {
         auto *c = new DeviceContext();
-        c->device = dev;
-        DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, dev),
-                       "cudaDeviceGetAttribute");
-        for (int i = 0; i < 2; i++) {
-            DRIFT_CUDA_TRY(cudaStreamCreateWithFlags(&c->streams[i], cudaStreamNonBlocking),
-                           "cudaStreamCreate");
-            DRIFT_CUDA_TRY(cudaEventCreateWithFlags(&c->done[i], cudaEventDisableTiming),
-                           "cudaEventCreate");
+        int rc = c->init(dev);
+        if (rc) {
+            c->release();
+            delete c;
+            return rc;
         }
         g_ctx[dev] = c;
     }
     *out = g_ctx[dev];
     return DRIFT_SUCCESS;
 }
+
+int DeviceContext::init(int dev)
+{
+    device = dev;
+    DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, dev),
+                   "cudaDeviceGetAttribute");
+    for (int i = 0; i < 2; i++) {
+        DRIFT_CUDA_TRY(cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+        DRIFT_CUDA_TRY(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    return DRIFT_SUCCESS;
+}
+
+// Makes `device` current for one scope and restores the caller's device.
+struct ScopedDevice {
+    int saved = -1;
+    bool switched = false;
+    explicit ScopedDevice(int device)
+    {
+        if (cudaGetDevice(&saved) == cudaSuccess && saved != device) switched = cudaSetDevice(device) == cudaSuccess;
+        cudaGetLastError();
+    }
+    ~ScopedDevice()
+    {
+        if (switched) cudaSetDevice(saved);
+    }
+};
 
 bool is_finite_value(double v) { return std::isfinite(v); }
 
@@ -756,6 +821,12 @@ int drift_host_free(void *ptr)
     return DRIFT_SUCCESS;
 }
 
+}  // extern "C"
+
+static int host_integrate(DeviceContext *ctx, const drift_launch *L);
+
+extern "C" {
+
 int drift_integrate_host(const drift_launch *L)
 {
     int rc = validate(L, false);
@@ -763,6 +834,15 @@ int drift_integrate_host(const drift_launch *L)
     DeviceContext *ctx = nullptr;
     rc = current_context(&ctx);
     if (rc) return rc;
+    return host_integrate(ctx, L);
+}
+
+}  // extern "C"
+
+// The host path on a given context (its device current, the launch valid).
+static int host_integrate(DeviceContext *ctx, const drift_launch *L)
+{
+    int rc = DRIFT_SUCCESS;
     std::lock_guard<std::mutex> lock(ctx->mu);
 
     const int64_t n = L->n;
@@ -904,6 +984,69 @@ int drift_integrate_host(const drift_launch *L)
         DRIFT_CUDA_TRY(cudaMemcpyAsync(L->n_rejected, ctx->rej.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s0), "D2H rejected");
     DRIFT_CUDA_TRY(cudaStreamSynchronize(s0), "cudaStreamSynchronize");
     DRIFT_CUDA_TRY(cudaStreamSynchronize(ctx->streams[1]), "cudaStreamSynchronize");
+    return DRIFT_SUCCESS;
+}
+
+struct drift_context {
+    DeviceContext c;
+};
+
+extern "C" {
+
+int drift_context_create(int32_t device, drift_context **out)
+{
+    if (!out) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_context_create: out is NULL");
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+        cudaGetLastError();
+        return fail(DRIFT_ERROR_NO_DEVICE, "no CUDA device");
+    }
+    int dev = device;
+    if (dev < 0 && cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(DRIFT_ERROR_NO_DEVICE, "no current CUDA device");
+    }
+    if (dev >= count) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "no such CUDA device");
+    ScopedDevice on(dev);
+    auto *ctx = new drift_context();
+    int rc = ctx->c.init(dev);
+    if (rc) {
+        ctx->c.release();
+        delete ctx;
+        return rc;
+    }
+    *out = ctx;
+    return DRIFT_SUCCESS;
+}
+
+int drift_context_integrate_host(drift_context *ctx, const drift_launch *L)
+{
+    if (!ctx) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_context_integrate_host: context is NULL");
+    int rc = validate(L, false);
+    if (rc) return rc;
+    ScopedDevice on(ctx->c.device);
+    return host_integrate(&ctx->c, L);
+}
+
+int drift_context_memory(drift_context *ctx, size_t *device_bytes, size_t *pinned_bytes)
+{
+    if (!ctx) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "drift_context_memory: context is NULL");
+    std::lock_guard<std::mutex> lock(ctx->c.mu);
+    if (device_bytes) *device_bytes = ctx->c.device_bytes();
+    if (pinned_bytes) *pinned_bytes = ctx->c.pinned_bytes();
+    return DRIFT_SUCCESS;
+}
+
+int drift_context_destroy(drift_context *ctx)
+{
+    if (!ctx) return DRIFT_SUCCESS;
+    {
+        std::lock_guard<std::mutex> lock(ctx->c.mu);
+        ScopedDevice on(ctx->c.device);
+        ctx->c.release();
+    }
+    delete ctx;
     return DRIFT_SUCCESS;
 }
 

@@ -255,6 +255,24 @@ int drift_integrate(const drift_launch *launch, void *stream);
  * particle chunks whose copies overlap the integration of other chunks. */
 int drift_integrate_host(const drift_launch *launch);
 
+/* Explicit host-path contexts.  drift_integrate_host uses one implicit
+ * context per device, created on first use and kept until the process exits,
+ * whose grow-only buffers can hold gigabytes after a large request.  An
+ * explicit context owns its own streams and buffers:
+ * drift_context_destroy frees them, and host threads with separate contexts
+ * run host-path integrations on one device concurrently (calls on one
+ * context are serialised).  The reference creates and drops a CUDA context
+ * on every call instead (src/dispatch/gpu/cuda_oxide.rs:16-28).
+ * device < 0 selects the caller's current device. */
+typedef struct drift_context drift_context;
+int drift_context_create(int32_t device, drift_context **context);
+/* drift_integrate_host on the context's device, streams and buffers. */
+int drift_context_integrate_host(drift_context *context, const drift_launch *launch);
+/* Device and page-locked host bytes the context's buffers hold now. */
+int drift_context_memory(drift_context *context, size_t *device_bytes, size_t *pinned_bytes);
+/* Waits for the context's work and frees it; NULL is a no-op. */
+int drift_context_destroy(drift_context *context);
+
 /* Largest number of requests one drift_integrate_batch launch carries. */
 #define DRIFT_MAX_BATCH 64
 

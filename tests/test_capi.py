@@ -181,3 +181,15 @@ def test_force_model_with_too_many_parts_is_rejected():
     L, keep = _model_launch(m)
     assert capi.lib().drift_integrate(ctypes.byref(L), None) == 1
     assert "at most 11" in capi.lib().drift_last_error().decode()
+
+
+INVALID_ARGUMENT = 1  # DRIFT_ERROR_INVALID_ARGUMENT
+
+
+def test_context_entry_points_validate_their_arguments():
+    lib = capi.lib()
+    assert lib.drift_context_create(0, None) == INVALID_ARGUMENT
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 1, 2, rtol=1e-10, atol=1e-10)
+    assert lib.drift_context_integrate_host(None, ctypes.byref(L)) == INVALID_ARGUMENT
+    assert lib.drift_context_memory(None, None, None) == INVALID_ARGUMENT
+    assert lib.drift_context_destroy(None) == 0
