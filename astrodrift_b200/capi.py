@@ -21,6 +21,7 @@ POT_KEPLER, POT_PLUMMER, POT_BOVY, POT_KEPLER_CARTESIAN, POT_MODEL = 0, 1, 2, 3,
 MAX_COMPONENTS = 11
 MAX_BATCH = 64  # DRIFT_MAX_BATCH: requests one batched launch carries
 EXACT, FMA = 0, 1
+Y0_ROWS, Y0_COLUMNS = 0, 1
 PLAIN, PERSISTENT, ORDERED = 0, 1, 2
 INITIAL_STEP_SENTINEL = -9999.99
 (PARTICLE_OK, PARTICLE_MIN_STEP, PARTICLE_MAX_STEPS, PARTICLE_NONFINITE, PARTICLE_TIMEOUT,
@@ -158,6 +159,9 @@ class DriftLaunch(ctypes.Structure):
         ("force_model", ctypes.POINTER(DriftForceModel)),
         ("arbitrary_times", ctypes.c_int32),
         ("tape_stride", ctypes.c_int32),
+        ("y0_layout", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("y0_stride", ctypes.c_int64),
     ]
 
 
@@ -332,14 +336,19 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
                    dt_one: float = INITIAL_STEP_SENTINEL, max_steps: int = 0,
                    timeout_s: float = 0.0, want_out: bool = True, out=None,
                    model: DriftForceModel | None = None, arbitrary_times: bool = False,
-                   context: "Context | None" = None) -> dict:
+                   context: "Context | None" = None, columns: bool = False) -> dict:
     """drift_integrate_host: host arrays in, host arrays out.  With `model`
     (whose origin table is a host array), `pot` is ignored and the stage
     integrates in the summed force.  With `context`, the call runs on that
     explicit context (drift_context_integrate_host) instead of the device's
-    implicit one."""
-    y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
-    n = y0.shape[0]
+    implicit one.  ``columns``: y0 is given as (6, n) columns
+    (DRIFT_Y0_COLUMNS) instead of (n, 6) rows."""
+    if columns:
+        y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(6, -1)
+        n = y0.shape[1]
+    else:
+        y0 = np.ascontiguousarray(y0, dtype=np.float64).reshape(-1, 6)
+        n = y0.shape[0]
     if ts is not None:
         ts = np.ascontiguousarray(ts, dtype=np.float64)
         nt = len(ts)
@@ -353,6 +362,8 @@ def integrate_host(method: int, pot: DriftPotential, y0, *, ts=None, t_end=None,
         L.potential = model_potential()
         L.force_model = ctypes.pointer(model)
     L.arbitrary_times = int(arbitrary_times)
+    if columns:
+        L.y0_layout, L.y0_stride = Y0_COLUMNS, n
     if want_out and out is None:
         out = np.empty((nt, n, 6))
     res = dict(

@@ -280,14 +280,20 @@ int validate(const drift_launch *L, bool device_pointers)
     if (L->nt < 2 || L->nt > INT32_MAX - 1)
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "nt must be in [2, 2^31 - 2]");
     if (!L->y0) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0 is NULL");
+    if (L->y0_layout != DRIFT_Y0_ROWS && L->y0_layout != DRIFT_Y0_COLUMNS)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown y0_layout");
+    if (L->y0_layout == DRIFT_Y0_COLUMNS && L->y0_stride != 0 && L->y0_stride < L->n)
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0_stride must be 0 or at least n");
     if (!L->ts && !L->t_end) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "either ts or t_end is required");
     if (!L->ts && !is_finite_value(L->t0)) return fail(DRIFT_ERROR_INVALID_ARGUMENT, "t0 must be finite");
     if (!is_finite_value(L->rtol_ln) || !is_finite_value(L->atol_ln))
         return fail(DRIFT_ERROR_INVALID_ARGUMENT, "tolerances must be finite logarithms");
     if (device_pointers &&
-        (reinterpret_cast<uintptr_t>(L->y0) % 16 || (L->out && reinterpret_cast<uintptr_t>(L->out) % 16) ||
+        (reinterpret_cast<uintptr_t>(L->y0) % (L->y0_layout == DRIFT_Y0_ROWS ? 16 : 8) ||
+         (L->out && reinterpret_cast<uintptr_t>(L->out) % 16) ||
          (L->y_final && reinterpret_cast<uintptr_t>(L->y_final) % 16)))
-        return fail(DRIFT_ERROR_INVALID_ARGUMENT, "y0, out and y_final must be 16-byte aligned");
+        return fail(DRIFT_ERROR_INVALID_ARGUMENT,
+                    "y0 (rows), out and y_final must be 16-byte aligned, y0 columns 8-byte aligned");
     if (L->tape) {
         if (!device_pointers)
             return fail(DRIFT_ERROR_INVALID_ARGUMENT, "the step tape is a device buffer (device entry points only)");
@@ -342,6 +348,7 @@ drift::KernelArgs make_args(const drift_launch *L)
     a.arbitrary_times = L->arbitrary_times != 0;
     a.tape_stride = L->tape_stride;
     a.sparse_output = L->nt <= drift::SPARSE_OUTPUT_NT;
+    a.y0_stride = L->y0_layout == DRIFT_Y0_COLUMNS ? (L->y0_stride ? L->y0_stride : L->n) : 0;
     a.potential = L->potential;
     if (L->potential.kind == DRIFT_POT_BOVY)
         drift::fill_bulge_table(1.5 - 0.5 * L->potential.bulge_alpha, &a.bulge);
@@ -460,6 +467,7 @@ int launch_batch(int sm_count, const drift_launch *R, int32_t count, void *ws, c
         S.first = first;
         S.n = R[i].n;
         S.y0 = R[i].y0;
+        S.y0_stride = R[i].y0_layout == DRIFT_Y0_COLUMNS ? (R[i].y0_stride ? R[i].y0_stride : R[i].n) : 0;
         S.ts = R[i].ts;
         S.t0 = R[i].t0;
         S.t_end = R[i].t_end;
@@ -903,7 +911,16 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
             model_dev.origins = ctx->origins.as<double>();
         }
     }
-    DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->y0.ptr, L->y0, n * row, cudaMemcpyHostToDevice, s0), "H2D y0");
+    const bool columns = L->y0_layout == DRIFT_Y0_COLUMNS;
+    if (columns) {
+        // six columns, packed to a stride of n on the device
+        const size_t spitch = (size_t)(L->y0_stride ? L->y0_stride : n) * sizeof(double);
+        DRIFT_CUDA_TRY(cudaMemcpy2DAsync(ctx->y0.ptr, n * sizeof(double), L->y0, spitch, n * sizeof(double), 6,
+                                         cudaMemcpyHostToDevice, s0),
+                       "H2D y0 columns");
+    } else {
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->y0.ptr, L->y0, n * row, cudaMemcpyHostToDevice, s0), "H2D y0");
+    }
     DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->grid.ptr, L->ts ? (const void *)L->ts : (const void *)L->t_end,
                                    grid_bytes, cudaMemcpyHostToDevice, s0),
                    "H2D grid");
@@ -936,7 +953,8 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
         drift_launch sub = *L;
         sub.n = cn;
         if (L->potential.kind == DRIFT_POT_MODEL) sub.force_model = &model_dev;
-        sub.y0 = ctx->y0.as<double>() + c0 * 6;
+        sub.y0 = columns ? ctx->y0.as<double>() + c0 : ctx->y0.as<double>() + c0 * 6;
+        sub.y0_stride = columns ? n : 0;
         sub.ts = L->ts ? ctx->grid.as<double>() : nullptr;
         sub.t_end = L->ts ? nullptr : ctx->grid.as<double>() + c0;
         sub.out = L->out ? ctx->out[slot].as<double>() : nullptr;

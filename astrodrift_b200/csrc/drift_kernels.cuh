@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
 
     auto start = [&](int64_t p) {
         const double *y0p;
+        int64_t stride;
         if (a.nsegs) {
             seg = segment_of(a, p);
             const Segment &S = a.segs[seg];
@@ -150,20 +151,27 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
             out.y_final = S.y_final;
             out.n = S.n;
             out.nt = S.nt;
-            y0p = S.y0 + p * 6;
+            stride = S.y0_stride;
+            y0p = stride ? S.y0 + p : S.y0 + p * 6;
         } else {
             if (!a.ts) grid.t_end = __ldg(a.t_end + p);
-            y0p = a.y0 + p * 6;
+            stride = a.y0_stride;
+            y0p = stride ? a.y0 + p : a.y0 + p * 6;
         }
         pid = p;
         out.pid = p;
         double y0[6];
-        const double2 *src = reinterpret_cast<const double2 *>(y0p);
+        if (stride) {
 #pragma unroll
-        for (int i = 0; i < 3; i++) {
-            double2 v = __ldg(src + i);
-            y0[2 * i] = v.x;
-            y0[2 * i + 1] = v.y;
+            for (int i = 0; i < 6; i++) y0[i] = __ldg(y0p + i * stride);
+        } else {
+            const double2 *src = reinterpret_cast<const double2 *>(y0p);
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                double2 v = __ldg(src + i);
+                y0[2 * i] = v.x;
+                y0[2 * i + 1] = v.y;
+            }
         }
         if (METHOD == DRIFT_DOP853)
             l853.begin(pot, y0, grid, a.rtol, a.atol, out);
@@ -304,18 +312,22 @@ __global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ Kerne
     const Pot pot = make_pot<Pot>(a, table);
     for (int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pid < a.n;
          pid += (int64_t)gridDim.x * blockDim.x) {
-        const double *y;
+        double y[6];
         double span, t_start;
         int64_t nt = a.nt;
+        auto load = [&](const double *base, int64_t stride, int64_t p) {
+#pragma unroll
+            for (int i = 0; i < 6; i++) y[i] = stride ? base[p + i * stride] : base[p * 6 + i];
+        };
         if (a.nsegs) {
             const Segment &S = a.segs[segment_of(a, pid)];
             const int64_t p = pid - S.first;
-            y = S.y0 + p * 6;
+            load(S.y0, S.y0_stride, p);
             nt = S.nt;
             span = S.ts ? fabs(__ldg(S.ts + S.nt - 1) - __ldg(S.ts)) : fabs(__ldg(S.t_end + p) - S.t0);
             t_start = S.ts ? __ldg(S.ts) : S.t0;
         } else {
-            y = a.y0 + pid * 6;
+            load(a.y0, a.y0_stride, pid);
             span = a.ts ? fabs(__ldg(a.ts + a.nt - 1) - __ldg(a.ts)) : fabs(__ldg(a.t_end + pid) - a.t0);
             t_start = a.ts ? __ldg(a.ts) : a.t0;
         }

@@ -12,7 +12,7 @@
 namespace drift {
 
 // Requests one batched launch can carry; the table travels in the kernel's
-// parameter space (MAX_BATCH x 104 bytes), so no device table is needed.
+// parameter space (MAX_BATCH x 112 bytes), so no device table is needed.
 constexpr int MAX_BATCH = DRIFT_MAX_BATCH;  // from drift_b200.h
 
 // One request of a batched launch: particles [first, first + n) of the
@@ -20,7 +20,8 @@ constexpr int MAX_BATCH = DRIFT_MAX_BATCH;  // from drift_b200.h
 struct Segment {
     int64_t first;
     int64_t n;
-    const double *y0;         // (n, 6)
+    const double *y0;         // (n, 6) rows, or 6 columns of y0_stride
+    int64_t y0_stride;        // 0: rows; > 0: column stride (elements)
     const double *ts;         // shared grid of this request, or NULL
     double t0;                // per-particle grid start (ts == NULL)
     const double *t_end;      // (n) per-particle grid ends (ts == NULL)
@@ -43,7 +44,8 @@ constexpr int SPARSE_OUTPUT_NT = 8;
 // Everything a launch needs, passed by value as the kernel parameter.
 struct KernelArgs {
     int64_t n;
-    const double *y0;         // (n, 6)
+    const double *y0;         // (n, 6) rows, or 6 columns of y0_stride
+    int64_t y0_stride;        // 0: rows; > 0: column stride (elements)
     int32_t nt;
     int32_t persistent;       // 0: plain schedule, 1: persistent schedule
     const double *ts;         // shared grid or NULL

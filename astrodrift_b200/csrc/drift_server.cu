@@ -451,6 +451,8 @@ int drift_server_submit(drift_server *s, const drift_launch *request, uint64_t *
         L.method < DRIFT_DOPR54 || L.method > DRIFT_DOP853 || L.precision < 0 || L.precision > 1 ||
         L.potential.kind < DRIFT_POT_KEPLER || L.potential.kind > DRIFT_POT_KEPLER_CARTESIAN)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "invalid request");
+    if (L.y0_layout != DRIFT_Y0_ROWS)
+        return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "the server takes y0 as (n, 6) rows");
     auto r = std::make_unique<Request>();
     r->L = L;
     r->submitted = Clock::now();

@@ -125,6 +125,7 @@ int drift_autotune(const drift_launch *launch, int64_t sample, drift_tuning *bes
     }
     // scratch outputs and workspace for the sample
     drift_launch L = *launch;
+    if (L.y0_layout == DRIFT_Y0_COLUMNS && L.y0_stride == 0) L.y0_stride = L.n;  // the sample keeps the columns
     L.n = n;
     L.out = nullptr;
     L.y_final = nullptr;

@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define DRIFT_ABI_VERSION 4
+#define DRIFT_ABI_VERSION 5
 
 /* Sentinel that asks DOPR54 for galpy's RK4 initial-step estimate
  * (src/integrators/galpy/mod.rs:8). */
@@ -211,7 +211,18 @@ typedef struct {
      * m - 1 states between checkpoints: about 8 + 64 / m bytes per step
      * instead of 64, for one extra forward step per step. */
     int32_t tape_stride;
+    /* Layout of y0.  DRIFT_Y0_ROWS (0, default): (n, 6) rows
+     * [x, y, z, vx, vy, vz], the reference's InputState (src/state/mod.rs:7-25).
+     * DRIFT_Y0_COLUMNS: six columns of y0_stride doubles, component c of
+     * particle i at y0[c * y0_stride + i] (y0_stride 0 means n): one tensor
+     * per coordinate, as column-major hosts hold them.  The request server
+     * takes rows only. */
+    int32_t y0_layout;
+    int32_t reserved;
+    int64_t y0_stride;
 } drift_launch;
+
+enum { DRIFT_Y0_ROWS = 0, DRIFT_Y0_COLUMNS = 1 };
 
 #define DRIFT_MAX_TAPE_STRIDE 16
 

@@ -31,7 +31,7 @@ def test_every_declared_symbol_is_exported():
 
 def test_abi_version_and_messages():
     lib = capi.lib()
-    assert lib.drift_abi_version() == 4
+    assert lib.drift_abi_version() == 5
     assert lib.drift_result_string(0) == b"success"
     assert lib.drift_result_string(1) == b"invalid argument"
 
@@ -80,6 +80,8 @@ def test_struct_layout_matches_header(tmp_path):
          "recorded by DOP853 only"),
         (lambda L: (setattr(L, "tape", 4096), setattr(L, "tape_steps", 0)), "tape_steps"),
         (lambda L: (setattr(L, "tape", 4104), setattr(L, "tape_steps", 8)), "16-byte aligned"),
+        (lambda L: setattr(L, "y0_layout", 7), "unknown y0_layout"),
+        (lambda L: (setattr(L, "y0_layout", 1), setattr(L, "y0_stride", 3)), "y0_stride must be 0 or at least n"),
     ],
 )
 def test_invalid_launches_are_rejected_before_any_device_work(mutate, message):
