@@ -8,6 +8,8 @@
 //   Kepler (both forms): amp
 //   Plummer:             amp, b
 //   Bovy:                mn_amp, mn_a, mn_b, nfw_amp, nfw_a, bulge_k
+// Used by the adjoint only, which is compiled with contraction: powers,
+// logs, exps and reciprocals are the few-ulp forms of drift_math.cuh.
 // The formulas are the analytic derivatives of the forces in
 // drift_potentials.cuh (shared/src/potential.rs:126-176, 229-262 and the
 // galpy-cylindrical Kepler force of src/integrators/galpy/dopr54.rs:75-88,
@@ -78,11 +80,13 @@ struct BovyJac {
     double mn_amp, mn_a, mn_b;
     double nfw_amp, nfw_a;
     double bulge_s, bulge_rc2, bulge_k, bulge_gamma_s;
+    double inv_nfw_a, inv_rc2;  // reciprocals formed once
     const double *table;
     __device__ BovyJac(const drift_potential &p, const double *bulge_table)
         : mn_amp(p.mn_amp), mn_a(p.mn_a), mn_b(p.mn_b), nfw_amp(p.nfw_amp), nfw_a(p.nfw_a),
           bulge_s(1.5 - 0.5 * p.bulge_alpha), bulge_rc2(p.bulge_rc * p.bulge_rc), bulge_k(p.bulge_k),
-          bulge_gamma_s(p.bulge_gamma_s), table(bulge_table)
+          bulge_gamma_s(p.bulge_gamma_s), inv_nfw_a(1.0 / p.nfw_a),
+          inv_rc2(1.0 / (p.bulge_rc * p.bulge_rc)), table(bulge_table)
     {
     }
     __device__ __forceinline__ void vjp(double x, double y, double z, const double *w, double *jw,
@@ -94,12 +98,12 @@ struct BovyJac {
         // disk
         {
             double zeta2 = z * z + mn_b * mn_b;
-            double zeta = sqrt(zeta2);
-            double izeta = 1.0 / zeta;
+            double izeta = rsqrt(zeta2);
+            double zeta = zeta2 * izeta;
             double A = mn_a + zeta;
             double D = x * x + y * y + A * A;
-            double d15 = 1.0 / (D * sqrt(D));
-            double d25 = d15 / D;
+            double d15 = unit_pow_m1p5(D);
+            double d25 = d15 * fast_rcp(D);
             double gz = A * z * izeta;
             double gw = x * w[0] + y * w[1] + gz * w[2];
             double h = z * z / zeta2 + A * mn_b * mn_b * izeta * izeta * izeta;
@@ -113,26 +117,28 @@ struct BovyJac {
                                 3.0 * A * mn_b * izeta * d25 * gw);
         }
         if (r2 != 0.0) {
-            const double r = sqrt(r2);
-            const double ir3 = 1.0 / (r2 * r);
-            const double c3 = 3.0 * xw * ir3 / r2;
+            const double inv_r = rsqrt(r2);
+            const double r = r2 * inv_r;
+            const double ir3 = inv_r * inv_r * inv_r;
+            const double c3 = 3.0 * xw * ir3 * (inv_r * inv_r);
             // halo
             {
                 double apr = nfw_a + r;
-                double m = log(1.0 + r / nfw_a) - r / apr;
-                double e = xw * ir3 / (apr * apr);
+                double inv_apr = fast_rcp(apr);
+                double m = unit_log(1.0 + r * inv_nfw_a) - r * inv_apr;
+                double e = xw * ir3 * (inv_apr * inv_apr);
                 jw[0] += -nfw_amp * (m * (w[0] * ir3 - x * c3) + x * e);
                 jw[1] += -nfw_amp * (m * (w[1] * ir3 - y * c3) + y * e);
                 jw[2] += -nfw_amp * (m * (w[2] * ir3 - z * c3) + z * e);
                 dp[3] += -m * xw * ir3;
-                dp[4] += nfw_amp * xw / (r * nfw_a * apr * apr);
+                dp[4] += nfw_amp * xw * inv_r * inv_nfw_a * (inv_apr * inv_apr);
             }
             // bulge
             {
-                double u = r2 / bulge_rc2;
+                double u = r2 * inv_rc2;
                 double G = bulge_lower_gamma(table, bulge_s, u, bulge_gamma_s);
-                double Gp = exp((bulge_s - 1.0) * log(u) - u) * 2.0 * r / bulge_rc2;
-                double e = Gp * xw * ir3 / r;
+                double Gp = unit_exp((bulge_s - 1.0) * unit_log(u) - u) * 2.0 * r * inv_rc2;
+                double e = Gp * xw * ir3 * inv_r;
                 jw[0] += -bulge_k * (G * (w[0] * ir3 - x * c3) + x * e);
                 jw[1] += -bulge_k * (G * (w[1] * ir3 - y * c3) + y * e);
                 jw[2] += -bulge_k * (G * (w[2] * ir3 - z * c3) + z * e);
