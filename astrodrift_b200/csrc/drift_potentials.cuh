@@ -14,7 +14,8 @@
 //                   and rsqrt instead of the reference's divisions.
 // pow(., -1.5) and pow(., 1.5) go through the routines of drift_math.cuh
 // instead of a general pow: correctly rounded in the exact unit, within a
-// few ulps in the contraction unit.
+// few ulps in the contraction unit, which also takes the Bovy force's log
+// and exp from drift_math.cuh's series forms (unit_log, unit_exp).
 #pragma once
 
 #include "drift_math.cuh"
