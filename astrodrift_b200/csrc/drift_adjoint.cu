@@ -34,6 +34,7 @@
 #include "drift_dop853.cuh"
 #include "drift_jacobians.cuh"
 #include "drift_launch_args.cuh"
+#include "drift_trace.h"
 
 int drift_internal_fail(int code, const char *msg);
 
@@ -515,6 +516,7 @@ cudaError_t launch(const AdjointArgs &a, int grid, int block, cudaStream_t s)
 
 extern "C" int drift_integrate_adjoint(const drift_adjoint_launch *A, void *stream)
 {
+    drift::TraceRange trace("drift integrate adjoint");
     if (!A) return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "adjoint launch is NULL");
     if (A->method != DRIFT_DOP853)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "the adjoint supports DOP853");

@@ -20,6 +20,7 @@
 #include "drift_b200.h"
 #include "drift_bulge_table.h"
 #include "drift_launch_args.cuh"
+#include "drift_trace.h"
 
 namespace drift {
 void fill_bulge_table(double s, BulgeTable *t)
@@ -599,6 +600,7 @@ int drift_query_workspace(const drift_launch *launch, size_t *bytes)
 
 int drift_integrate(const drift_launch *launch, void *stream)
 {
+    drift::TraceRange trace("drift integrate");
     int rc = validate(launch, true);
     if (rc) return rc;
     DeviceContext *ctx = nullptr;
@@ -852,6 +854,7 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
 {
     int rc = DRIFT_SUCCESS;
     std::lock_guard<std::mutex> lock(ctx->mu);
+    drift::TraceRange trace("drift host integrate");
 
     const int64_t n = L->n;
     const int64_t nt = L->nt;
@@ -943,6 +946,7 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
     };
 
     for (int64_t c0 = 0; c0 < n; c0 += chunk, chunk_index++) {
+        drift::TraceRange chunk_trace("drift host chunk");
         const int slot = (int)(chunk_index & 1);
         cudaStream_t s = ctx->streams[slot];
         const int64_t cn = std::min(chunk, n - c0);
@@ -988,6 +992,7 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
         }
     }
     // Per-particle outputs once every chunk is done.
+    drift::TraceRange tail_trace("drift host copy-out and wait");
     DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[1], ctx->streams[1]), "cudaEventRecord");
     DRIFT_CUDA_TRY(cudaStreamWaitEvent(s0, ctx->done[1], 0), "cudaStreamWaitEvent");
     if (L->y_final)

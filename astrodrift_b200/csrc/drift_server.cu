@@ -29,6 +29,7 @@
 #include <vector>
 
 #include "drift_b200.h"
+#include "drift_trace.h"
 #include "drift_launch_args.cuh"
 
 // Internal launcher shared with drift_capi.cu.
@@ -303,6 +304,7 @@ struct drift_server {
             D.workspace = base;
             D.workspace_bytes = scratch;
         }
+        drift::TraceRange trace("drift server batch");
         int rc = drift_internal_launch_batch(launch_sms, sub.data(), (int32_t)sub.size(), base, s);
         for (size_t i = 0; i < batch->pieces.size(); i++) {
             Piece &p = batch->pieces[i];
