@@ -502,8 +502,58 @@ class Graph:
             pass
 
 
-def autotune(L: DriftLaunch, sample: int = 0) -> DriftTuning:
-    """drift_autotune: the fastest block size and schedule for launch L."""
+def _device_name() -> str:
+    try:
+        import torch
+
+        return torch.cuda.get_device_name(torch.cuda.current_device())
+    except Exception:
+        return "unknown"
+
+
+def _ceil_log2(v: int) -> int:
+    return max(int(v) - 1, 0).bit_length()
+
+
+def tuning_key(L: DriftLaunch) -> str:
+    """The workload class drift_autotune caches a choice under (method,
+    precision, potential, grid kind, ceil log2 of nt and n, arbitrary
+    times), prefixed with the GPU's name."""
+    return "|".join(str(v) for v in (_device_name(), L.method, L.precision, L.potential.kind,
+                                      int(bool(L.ts)), _ceil_log2(L.nt), _ceil_log2(L.n),
+                                      int(L.arbitrary_times)))
+
+
+def autotune(L: DriftLaunch, sample: int = 0, cache_path=None) -> DriftTuning:
+    """drift_autotune: the fastest block size and schedule for launch L.
+
+    The library caches choices for the life of the process.  With
+    ``cache_path`` (a JSON file) they also persist across processes: a
+    workload class found there is returned without timing (``cached`` = 2),
+    and a new choice is added to the file."""
+    import json
+    import os
+
+    key = tuning_key(L) if cache_path is not None else None
+    if cache_path is not None and os.path.exists(cache_path):
+        with open(cache_path) as f:
+            entry = json.load(f).get(key)
+        if entry is not None:
+            t = DriftTuning()
+            t.block_size, t.schedule = int(entry["block_size"]), int(entry["schedule"])
+            t.seconds, t.sample, t.cached = float(entry["seconds"]), int(entry["sample"]), 2
+            return t
     t = DriftTuning()
     check(lib().drift_autotune(ctypes.byref(L), sample, ctypes.byref(t)), "drift_autotune")
+    if cache_path is not None:
+        table = {}
+        if os.path.exists(cache_path):
+            with open(cache_path) as f:
+                table = json.load(f)
+        table[key] = {"block_size": t.block_size, "schedule": t.schedule, "seconds": t.seconds,
+                      "sample": t.sample}
+        tmp = f"{cache_path}.tmp{os.getpid()}"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache_path)
     return t

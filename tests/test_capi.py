@@ -195,3 +195,22 @@ def test_context_entry_points_validate_their_arguments():
     assert lib.drift_context_integrate_host(None, ctypes.byref(L)) == INVALID_ARGUMENT
     assert lib.drift_context_memory(None, None, None) == INVALID_ARGUMENT
     assert lib.drift_context_destroy(None) == 0
+
+
+def test_tuning_choices_persist_in_a_json_file(tmp_path, monkeypatch):
+    import json
+
+    monkeypatch.setattr(capi, "_device_name", lambda: "NVIDIA B200")
+    L = capi.make_launch(capi.DOP853, capi.plummer(), 150000, 201, rtol=1e-12, atol=1e-12)
+    L.ts = 4096  # a shared grid (the key only looks at its presence)
+    key = capi.tuning_key(L)
+    assert key == "NVIDIA B200|1|0|1|1|8|18|0"  # DOP853, exact, Plummer, shared grid, nt<=2^8, n<=2^18
+    path = tmp_path / "tuning.json"
+    path.write_text(json.dumps({key: {"block_size": 96, "schedule": 2, "seconds": 0.25, "sample": 16384}}))
+
+    def no_timing():
+        raise AssertionError("a cached class must not be timed again")
+
+    monkeypatch.setattr(capi, "lib", no_timing)
+    t = capi.autotune(L, cache_path=str(path))
+    assert (t.block_size, t.schedule, t.cached, t.sample) == (96, 2, 2, 16384)

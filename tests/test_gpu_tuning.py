@@ -99,3 +99,23 @@ def test_autotune_picks_work_stealing_for_uneven_workloads_and_caches(cuda_devic
     got = capi.integrate_host(capi.DOP853, capi.plummer(1.0, 1.0), y0[:2000], t_end=t_end[:2000], nt=5,
                               rtol=1e-10, atol=1e-10, schedule=t.schedule, block_size=t.block_size)
     np.testing.assert_array_equal(got["out"], ref["out"])
+
+
+def test_autotune_choice_persists_in_a_json_cache(cuda_device, tmp_path):
+    import json
+
+    import torch
+
+    dev = torch.device("cuda:0")
+    n = 4096
+    y0_d = torch.tensor(_plummer_ics(n, 9), device=dev)
+    ts_d = torch.tensor(np.linspace(0.0, 3.0, 7), device=dev)
+    L = capi.make_launch(capi.DOPR54, capi.plummer(1.0, 1.0), n, 7, rtol=1e-9, atol=1e-9)
+    L.y0, L.ts = y0_d.data_ptr(), ts_d.data_ptr()
+    path = tmp_path / "tuning.json"
+    first = capi.autotune(L, cache_path=str(path))
+    assert first.cached in (0, 1)  # timed now, or earlier in this process
+    table = json.loads(path.read_text())
+    assert table[capi.tuning_key(L)]["block_size"] == first.block_size
+    again = capi.autotune(L, cache_path=str(path))
+    assert again.cached == 2 and (again.block_size, again.schedule) == (first.block_size, first.schedule)
