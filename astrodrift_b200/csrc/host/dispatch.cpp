@@ -441,7 +441,7 @@ std::vector<py::object> gpu_dispatch(const Config &config, const IntegrationPlan
                   fmt("stage %d: %lld particles finished in %s", stage_no, (long long)n,
                       rust_duration(secs).c_str()));
         results.push_back(out);
-        if (stats) stats->push_back(StageStats{acc, rej, status, secs});
+        if (stats) stats->push_back(StageStats{acc, rej, status, secs, (uint64_t)in_bytes, (uint64_t)out_bytes});
     }
     const double elapsed =
         std::chrono::duration<double>(std::chrono::steady_clock::now() - started).count();

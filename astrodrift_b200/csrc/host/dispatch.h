@@ -35,7 +35,9 @@ struct StageStats {
     pybind11::array_t<uint32_t> accepted;
     pybind11::array_t<uint32_t> rejected;
     pybind11::array_t<uint8_t> status;
-    double seconds = 0.0;
+    double seconds = 0.0;        // the stage's wall time, copies included
+    uint64_t bytes_in = 0;       // initial states and grid copied to the device
+    uint64_t bytes_written = 0;  // trajectory bytes the stage produced
 };
 
 // Integrates every stage of `plan`; result[i] is the (nt, N, 6) trajectory

@@ -335,6 +335,8 @@ struct ConfigObject {
                         d["rejected"] = stats[s].rejected;
                         d["status"] = stats[s].status;
                         d["seconds"] = stats[s].seconds;
+                        d["bytes_in"] = stats[s].bytes_in;
+                        d["bytes_written"] = stats[s].bytes_written;
                         st = d;
                     }
                 }

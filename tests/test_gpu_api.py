@@ -109,6 +109,9 @@ def test_run_stats_report_step_counts(cuda_device) -> None:
     results, stats = sim.run(stats=True)
     assert stats[1] is None
     assert (stats[0]["accepted"] > 0).all() and (stats[0]["status"] == 0).all()
+    n = len(stats[0]["accepted"])
+    assert stats[0]["bytes_written"] == results[0].shape[0] * n * 6 * 8
+    assert stats[0]["bytes_in"] >= n * 6 * 8 and stats[0]["seconds"] > 0
 
 
 def test_plummer_and_bovy_backgrounds(cuda_device, oracle) -> None:
