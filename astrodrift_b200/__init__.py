@@ -17,26 +17,47 @@ from __future__ import annotations
 
 from .selectors import Engine, Implementation, Method
 
-try:
-    from . import _drift
-except ImportError as exc:  # pragma: no cover - exercised only without a build
-    raise ImportError(
-        "astrodrift_b200's native extension is not built; run "
-        "`python -m astrodrift_b200.build` (needs nvcc for sm_100a)"
-    ) from exc
+# Names served by the pybind11 host module.  It is loaded on first use, so
+# importing a pure-Python submodule (workloads, sharding) maps no native code.
+_NATIVE_NAMES = (
+    "Potential",
+    "Container",
+    "Config",
+    "particles",
+    "test_particles",
+    "background",
+    "DriftError",
+    "IntegrationError",
+)
 
-Potential = _drift.Potential
-Container = _drift.Container
-Config = _drift.Config
-particles = _drift.particles
-test_particles = _drift.test_particles
-background = _drift.background
-DriftError = _drift.DriftError
-IntegrationError = _drift.IntegrationError
 
-# Exceptions are part of the package's public surface.
-DriftError.__module__ = __name__
-IntegrationError.__module__ = __name__
+def _load_native():
+    try:
+        from . import _drift
+    except ImportError as exc:
+        raise ImportError(
+            "astrodrift_b200's native extension is not built; run "
+            "`python -m astrodrift_b200.build` (needs nvcc for sm_100a)"
+        ) from exc
+    # Exceptions are part of the package's public surface.
+    if _drift.DriftError.__module__ != "drift":
+        _drift.DriftError.__module__ = __name__
+        _drift.IntegrationError.__module__ = __name__
+    for name in _NATIVE_NAMES:
+        globals()[name] = getattr(_drift, name)
+    return _drift
+
+
+def __getattr__(name: str):
+    if name in _NATIVE_NAMES:
+        _load_native()
+        return globals()[name]
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
+
+
+def __dir__():
+    return sorted(set(globals()) | set(_NATIVE_NAMES))
+
 
 __all__ = [
     "Potential",

@@ -1,7 +1,7 @@
 """ctypes binding of the C ABI in ``include/drift_b200.h`` (``libdrift_b200.so``).
 
-This is the boundary a foreign-language host binds; the
-parity tests, the smoke check and the benchmark call the kernels through it.
+This is the boundary a foreign-language host binds; the parity tests, the
+smoke check and the benchmark call the kernels through it.
 Functions here raise ``RuntimeError`` with the library's message when a call
 fails; nothing falls back to a CPU implementation.
 """

@@ -629,25 +629,18 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[DRIFT_NOALLOC_S
 
 namespace {
 
-constexpr int NOALLOC_MAX_DEVICES = 64;
-std::mutex g_noalloc_mu;
-void *g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {nullptr};
-
-// Device address of g_noalloc_scratch on the current device, looked up once
-// per device.  In host code the array's name is only a host-side stand-in;
-// kernels must receive this address instead.
-int noalloc_scratch(int device, void **out)
+// Device address of g_noalloc_scratch in the calling thread's current
+// context.  In host code the array's name is only a host-side stand-in;
+// kernels must receive this address instead.  It is looked up on every call
+// (a host-side table lookup once the module is loaded, no allocation): an
+// address saved from an earlier call would be stale after a device reset or
+// under another context on the same device.
+int noalloc_scratch(void **out)
 {
-    if (device < 0 || device >= NOALLOC_MAX_DEVICES)
-        return fail(DRIFT_ERROR_NO_DEVICE, "drift_integrate_noalloc: device index out of range");
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_ptr[device]) {
-        void *ptr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
-        g_noalloc_ptr[device] = ptr;
-    }
-    *out = g_noalloc_ptr[device];
+    void *ptr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(no-alloc scratch)");
+    *out = ptr;
     return DRIFT_SUCCESS;
 }
 
@@ -670,7 +663,7 @@ extern "C" int drift_integrate_noalloc(const drift_launch *launch, void *stream)
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess) return fail(DRIFT_ERROR_NO_DEVICE, std::string("no CUDA device: ") + cudaGetErrorString(e));
     void *scratch = nullptr;
-    rc = noalloc_scratch(device, &scratch);
+    rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     int sm_count = 0;
     DRIFT_CUDA_TRY(cudaDeviceGetAttribute(&sm_count, cudaDevAttrMultiProcessorCount, device),

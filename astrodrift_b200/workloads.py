@@ -8,6 +8,39 @@ from __future__ import annotations
 
 import numpy as np
 
+# The Bovy-style composite of the benchmark configurations in natural units
+# (R0 = 1, v_c(1) = 1): power-law bulge with exponential cutoff (alpha, rc)
+# normalised to F_r(1) = -bulge_force, Miyamoto-Nagai disk and NFW halo with
+# the reference's fraction-normalised amplitudes (shared/src/potential.rs:103-112).
+BOVY_PARAMS = dict(alpha=1.8, rc=1.9 / 8.0, bulge_force=0.05, mn_amp=0.7574802019,
+                   mn_a=3.0 / 8.0, mn_b=0.28 / 8.0, nfw_amp=4.852230533528, nfw_a=16.0 / 8.0)
+
+
+def bovy_radial_force(R) -> np.ndarray:
+    """F_R(R, z = 0) of the composite with BOVY_PARAMS, in float64 on the host.
+
+    bulge  -k gamma(s, r^2 / rc^2) / r^2 with s = 3/2 - alpha/2 and k set so
+           that the bulge's F_r(1) = -bulge_force (gamma: scipy's regularised
+           lower incomplete gamma times Gamma(s));
+    disk   -amp R / (R^2 + (a + b)^2)^(3/2) in the plane;
+    halo   -amp (ln(1 + r/a) - r/(a + r)) / r^2.
+    The benchmark's initial conditions use it in every arm, so they are the
+    same whichever implementation integrates them.
+    """
+    from scipy.special import gamma, gammainc
+
+    p = BOVY_PARAMS
+    R = np.asarray(R, dtype=np.float64)
+    s = 1.5 - 0.5 * p["alpha"]
+    rc2 = p["rc"] ** 2
+    lower = lambda x: gammainc(s, x) * gamma(s)  # noqa: E731
+    k = p["bulge_force"] / lower(1.0 / rc2)
+    bulge = -k * lower(R * R / rc2) / (R * R)
+    disk = -p["mn_amp"] * R / (R * R + (p["mn_a"] + p["mn_b"]) ** 2) ** 1.5
+    a = p["nfw_a"]
+    halo = -p["nfw_amp"] * (np.log1p(R / a) - R / (a + R)) / (R * R)
+    return bulge + disk + halo
+
 
 def _isotropic(rng, n):
     u = rng.normal(size=(n, 3))
@@ -73,7 +106,10 @@ def bovy_disc(n: int, seed: int = 3, radial_force=None) -> tuple[np.ndarray, np.
     """Configuration 3: R log-uniform on [0.05, 20], phi ~ U[0, 2 pi),
     z ~ N(0, 0.1 R); v_c(R) = sqrt(R |F_R(R, 0)|); v_T = v_c (1 + 0.1 N(0,1)),
     v_R, v_z ~ N(0, 0.1 v_c); per-particle end times t_end ~ U[10, 1000].
-    `radial_force(R)` returns F_R(R, 0) of the composite."""
+    `radial_force(R)` returns F_R(R, 0) of the composite (default:
+    bovy_radial_force, on the host)."""
+    if radial_force is None:
+        radial_force = bovy_radial_force
     rng = np.random.default_rng(seed)
     R = np.exp(rng.uniform(np.log(0.05), np.log(20.0), n))
     phi = rng.uniform(0.0, 2.0 * np.pi, n)

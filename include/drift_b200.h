@@ -428,9 +428,11 @@ int drift_integrate_adjoint(const drift_adjoint_launch *adjoint, void *stream);
  *    DRIFT_NOALLOC_SCRATCH_BYTES is rejected with DRIFT_ERROR_WORKSPACE
  *    (plain and persistent requests always fit; ordered requests fit up to
  *    563 particles);
- *  - the first call on a device looks up the array's device address for
- *    that device (with that device current); make that first call before
- *    any CUDA stream capture;
+ *  - every call looks up the array's device address in the calling
+ *    thread's current context (the device the call runs on must be
+ *    current), so the address stays right after a device reset or under
+ *    another context; the first call on a device also loads the library's
+ *    kernels there, so make that first call before any CUDA stream capture;
  *  - every call shares the one array and clears the part that must start
  *    at zero before its launch, so calls whose kernels overlap on the GPU
  *    (different streams, or different host threads) race with each other:

@@ -69,6 +69,13 @@ double oracle_lower_gamma(double s, double x, double gamma_s)
     return gamma_s - prefactor * h;
 }
 
+/* The bulge force's incomplete gamma.  The operation counter (opcount.cpp)
+ * redefines this name to tally each evaluation as one special-function call,
+ * like pow, exp and log, since its loop lengths depend on the argument. */
+#ifndef ORACLE_BULGE_GAMMA
+#define ORACLE_BULGE_GAMMA oracle_lower_gamma
+#endif
+
 void oracle_bovy_setup(oracle_potential *p, double alpha, double rc, double force_at_1,
                        double mn_amp, double mn_a, double mn_b, double nfw_amp, double nfw_a)
 {
@@ -174,7 +181,7 @@ static void bulge(const oracle_potential *p, double x, double y, double z, doubl
     }
     double r = sqrt(r2);
     double s = 1.5 - 0.5 * p->bulge_alpha;
-    double g = oracle_lower_gamma(s, r2 / (p->bulge_rc * p->bulge_rc), p->bulge_gamma_s);
+    double g = ORACLE_BULGE_GAMMA(s, r2 / (p->bulge_rc * p->bulge_rc), p->bulge_gamma_s);
     double ar_over_r = -p->bulge_k * g / (r2 * r);
     *ax = ar_over_r * x;
     *ay = ar_over_r * y;

