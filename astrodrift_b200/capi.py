@@ -61,6 +61,7 @@ EXPORTED = (
     "drift_server_submit",
     "drift_server_wait",
     "drift_server_stats_get",
+    "drift_server_cancel",
     "drift_server_destroy",
     "drift_integrate_adjoint",
     "drift_origin_table",

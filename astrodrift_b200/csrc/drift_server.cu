@@ -1,18 +1,26 @@
 // drift_server.cu -- resident request server with continuous batching.
 //
-// A scheduler thread owns a device memory pool, a set of streams and the
-// queue of submitted requests.  Whenever a stream is free it forms a batch:
-// the oldest pending request plus every later pending request that can share
-// its launch (same method, precision, schedule, potential, tolerances and
-// limits), as long as the batch fits the device-memory budget.  A request larger than the
-// remaining budget is admitted in particle chunks.  Each batch copies its
-// inputs in, runs one batched integration launch (drift_integrate_batch's
-// kernel path), copies trajectories and per-particle outputs back into the
-// requests' host buffers and frees its memory, all ordered on its stream, so
-// requests that arrive while others are on the GPU start as soon as a stream
-// and memory free up and their kernels overlap the running ones.  Completion
-// is signalled from the stream (cudaLaunchHostFunc) to the scheduler, which
-// wakes waiters.  No counterpart exists in the reference.
+// A scheduler thread owns the queue of submitted requests and a device
+// memory pool; one worker thread per stream runs the batches.  Whenever a
+// stream is free the scheduler forms a batch: the oldest pending request plus
+// every later pending request that can share its launch (same method,
+// precision, schedule, potential, tolerances and limits), as long as the
+// batch fits the device-memory budget.  A request larger than the remaining
+// budget is admitted in particle chunks.  The stream's worker then copies
+// the batch's inputs in, runs one batched integration launch
+// (drift_integrate_batch's kernel path), copies trajectories and
+// per-particle outputs back into the requests' host buffers, frees its
+// memory and waits for its stream, so requests that arrive while others are
+// on the GPU start as soon as a stream and memory free up and their kernels
+// overlap the running ones.
+//
+// Locking: the mutex guards the queue, the requests' bookkeeping and the
+// statistics, and no thread holds it across a CUDA call.  A worker blocked
+// in a copy into pageable host memory (which returns only when its kernel
+// has finished) or in its stream wait holds up nobody but its own stream:
+// the scheduler keeps admitting batches on the other streams, and submit,
+// wait, cancel and stats calls proceed.  No counterpart exists in the
+// reference.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -52,6 +60,7 @@ struct Request {
     int64_t finished = 0;      // particles whose batch completed
     int result = DRIFT_SUCCESS;
     bool done = false;
+    bool cancelled = false;    // no further particles are admitted
     Clock::time_point submitted, completed;
 };
 
@@ -65,9 +74,11 @@ struct Piece {
 struct Batch {
     int slot = -1;
     void *dmem = nullptr;
-    size_t bytes = 0;
+    size_t bytes = 0;           // device bytes (scratch + pieces)
+    size_t scratch = 0;         // scratch bytes at the front of dmem
+    int schedule = DRIFT_SCHEDULE_PERSISTENT;
+    int launch_sms = 0;
     std::vector<Piece> pieces;
-    std::atomic<bool> complete{false};
 };
 
 // Bytes a chunk of cn particles of request L needs on the device.
@@ -120,71 +131,72 @@ struct drift_server {
     size_t budget = 0;
     cudaMemPool_t pool = nullptr;
     std::vector<cudaStream_t> streams;
-    std::vector<bool> slot_busy;
+
+    // One worker per stream; `job` is handed over under mu.
+    struct Worker {
+        std::thread thread;
+        std::condition_variable cv;
+        std::unique_ptr<Batch> job;
+        bool busy = false;       // a batch is planned for or running on this stream
+    };
+    std::vector<std::unique_ptr<Worker>> workers;
 
     std::mutex mu;
     std::condition_variable cv_work;  // scheduler wake-up
     std::condition_variable cv_done;  // waiters
     std::deque<Request *> pending;
     std::map<uint64_t, std::unique_ptr<Request>> requests;
-    std::vector<std::unique_ptr<Batch>> inflight;
     size_t bytes_inflight = 0;
+    int batches_inflight = 0;
     uint64_t next_ticket = 1;
-    bool stop = false;
-    std::thread worker;
-    std::string last_error;
+    bool stop = false;          // no further admissions (destroy)
+    bool quit = false;          // workers exit once idle
+    std::thread scheduler;
 
     drift_server_stats stats{};
 
-    static void CUDART_CB on_batch_done(void *p)
+    // With mu held: a request ends once every particle it will run has
+    // finished (all of them, or the admitted ones after a cancellation).
+    void maybe_complete(Request *r)
     {
-        auto *pair = static_cast<std::pair<drift_server *, Batch *> *>(p);
-        drift_server *s = pair->first;
-        {
-            std::lock_guard<std::mutex> lock(s->mu);
-            pair->second->complete = true;
-        }
-        s->cv_work.notify_all();
-        delete pair;
+        if (r->done) return;
+        const int64_t target = r->cancelled ? r->admitted : r->L.n;
+        if (r->finished < target) return;
+        if (r->cancelled) r->result = DRIFT_ERROR_CANCELLED;
+        r->done = true;
+        r->completed = Clock::now();
+        stats.requests_completed++;
+        stats.particles_completed += r->finished;
+        cv_done.notify_all();
     }
 
-    // Called with mu held: retire completed batches.
-    void retire()
+    // With mu held: the pieces of a batch that never ran go back to their
+    // requests (the scheduler plans one batch at a time, so they are the
+    // last particles admitted of each request).
+    void give_back(Batch &b)
     {
-        for (size_t i = 0; i < inflight.size();) {
-            Batch *b = inflight[i].get();
-            if (!b->complete) {
-                i++;
-                continue;
-            }
-            for (Piece &p : b->pieces) {
-                p.req->finished += p.cn;
-                if (p.req->finished == p.req->L.n && !p.req->done) {
-                    p.req->done = true;
-                    p.req->completed = Clock::now();
-                    stats.requests_completed++;
-                    stats.particles_completed += p.req->L.n;
-                }
-            }
-            bytes_inflight -= b->bytes;
-            slot_busy[b->slot] = false;
-            inflight.erase(inflight.begin() + i);
-            cv_done.notify_all();
+        for (auto it = b.pieces.rbegin(); it != b.pieces.rend(); ++it) {
+            Request *r = it->req;
+            r->admitted = it->c0;
+            if (!r->cancelled && std::find(pending.begin(), pending.end(), r) == pending.end())
+                pending.push_front(r);
+            maybe_complete(r);
         }
     }
 
-    // Called with mu held: form and launch one batch on a free slot.
-    // Returns false when nothing could be admitted.
-    bool admit()
+    // With mu held: form one batch for a free stream.  Its pieces are taken
+    // from the queue and its bytes reserved; returns nullptr when nothing can
+    // be admitted now.
+    std::unique_ptr<Batch> plan()
     {
-        int slot = -1;
-        for (int i = 0; i < (int)slot_busy.size(); i++)
-            if (!slot_busy[i]) {
-                slot = i;
+        int free_slot = -1;
+        for (int i = 0; i < (int)workers.size(); i++)
+            if (!workers[i]->busy) {
+                free_slot = i;
                 break;
             }
-        if (slot < 0 || pending.empty()) return false;
-        slot = -1;  // chosen once the batch's size is known
+        while (!pending.empty() && pending.front()->cancelled) pending.pop_front();
+        if (free_slot < 0 || pending.empty()) return nullptr;
         Request *head = pending.front();
         auto batch = std::make_unique<Batch>();
         size_t room = budget > bytes_inflight ? budget - bytes_inflight : 0;
@@ -195,7 +207,7 @@ struct drift_server {
         for (Request *r : pending) {
             if ((int)batch->pieces.size() >= drift::MAX_BATCH) break;
             if (particles >= opts.max_batch_particles) break;
-            if (!compatible(head->L, r->L)) continue;
+            if (r->cancelled || !compatible(head->L, r->L)) continue;
             int64_t remaining = r->L.n - r->admitted;
             int64_t cn = std::min<int64_t>(remaining, opts.max_batch_particles - particles);
             // shrink to the memory that is left
@@ -203,148 +215,162 @@ struct drift_server {
                 cn = cn > 256 ? cn / 2 : cn - 1;
             if (cn <= 0) {
                 if (r == head) {
-                    if (inflight.empty() && scratch_bytes(schedule, 1) + piece_bytes(r->L, 1) > budget) {
+                    if (batches_inflight == 0 && scratch_bytes(schedule, 1) + piece_bytes(r->L, 1) > budget) {
                         // Not even one particle fits the whole budget.
                         r->result = DRIFT_ERROR_OUT_OF_MEMORY;
                         r->done = true;
                         r->completed = Clock::now();
                         pending.pop_front();
                         cv_done.notify_all();
-                        return !pending.empty();
+                        return plan();
                     }
                     break;  // keep FIFO order for the head: wait for memory
                 }
                 continue;
             }
-            Piece p{};
-            p.req = r;
-            p.c0 = r->admitted;
-            p.cn = cn;
+            Piece pc{};
+            pc.req = r;
+            pc.c0 = r->admitted;
+            pc.cn = cn;
             size_t off = used;
-            p.off_y0 = off;
+            pc.off_y0 = off;
             off += align_up(cn * 48);
-            p.off_grid = off;
+            pc.off_grid = off;
             off += align_up(r->L.ts ? r->L.nt * sizeof(double) : cn * sizeof(double));
-            p.off_out = off;
+            pc.off_out = off;
             if (r->L.out) off += align_up((size_t)r->L.nt * cn * 48);
-            p.off_fin = off;
+            pc.off_fin = off;
             if (r->L.y_final) off += align_up(cn * 48);
-            p.off_st = off;
+            pc.off_st = off;
             if (r->L.status) off += align_up(cn);
-            p.off_err = off;
+            pc.off_err = off;
             if (r->L.err_code) off += align_up(cn * 4);
-            p.off_acc = off;
+            pc.off_acc = off;
             if (r->L.n_accepted) off += align_up(cn * 4);
-            p.off_rej = off;
+            pc.off_rej = off;
             if (r->L.n_rejected) off += align_up(cn * 4);
             used = off;
             r->admitted += cn;
             particles += cn;
-            batch->pieces.push_back(p);
+            batch->pieces.push_back(pc);
             if (r->admitted == r->L.n) taken.push_back(r);
             if (r != head && cn < remaining) break;
         }
-        if (batch->pieces.empty()) return false;
+        if (batch->pieces.empty()) return nullptr;
         for (Request *r : taken) pending.erase(std::find(pending.begin(), pending.end(), r));
         const size_t scratch = scratch_bytes(schedule, particles);
-        for (Piece &p : batch->pieces)
-            for (size_t *o : {&p.off_y0, &p.off_grid, &p.off_out, &p.off_fin, &p.off_st, &p.off_err,
-                              &p.off_acc, &p.off_rej})
+        for (Piece &pc : batch->pieces)
+            for (size_t *o : {&pc.off_y0, &pc.off_grid, &pc.off_out, &pc.off_fin, &pc.off_st, &pc.off_err,
+                              &pc.off_acc, &pc.off_rej})
                 *o += scratch;
         used += scratch;
 
         // Small batches run on the high-priority stream 0 and may use every
         // SM; large ones use the other streams and leave the reserve free.
         const bool small = particles <= small_particles;
-        if (small && !slot_busy[0]) slot = 0;
-        for (int i = 1; slot < 0 && i < (int)slot_busy.size(); i++)
-            if (!slot_busy[i]) slot = i;
+        int slot = -1;
+        if (small && !workers[0]->busy) slot = 0;
+        for (int i = 1; slot < 0 && i < (int)workers.size(); i++)
+            if (!workers[i]->busy) slot = i;
         if (slot < 0) slot = 0;  // only stream 0 is free
-        const int launch_sms = small ? sm_count : std::max(1, sm_count - reserve_sms);
-
-        cudaStream_t s = streams[slot];
-        void *dmem = nullptr;
-        if (cudaMallocFromPoolAsync(&dmem, used, pool, s) != cudaSuccess) {
-            cudaGetLastError();
-            // give the pieces back and wait for memory
-            for (Piece &p : batch->pieces) p.req->admitted = p.c0;
-            for (auto it = taken.rbegin(); it != taken.rend(); ++it) pending.push_front(*it);
-            return false;
-        }
         batch->slot = slot;
-        batch->dmem = dmem;
         batch->bytes = used;
-        char *base = static_cast<char *>(dmem);
+        batch->scratch = scratch;
+        batch->schedule = schedule;
+        batch->launch_sms = small ? sm_count : std::max(1, sm_count - reserve_sms);
+        workers[slot]->busy = true;
+        bytes_inflight += used;
+        batches_inflight++;
+        return batch;
+    }
 
-        std::vector<drift_launch> sub(batch->pieces.size());
-        for (size_t i = 0; i < batch->pieces.size(); i++) {
-            Piece &p = batch->pieces[i];
-            const drift_launch &L = p.req->L;
+    // Without mu: every CUDA call of one batch on its stream, ending with a
+    // wait for the stream.  Returns the batch's drift_result.
+    int execute(Batch &b)
+    {
+        cudaStream_t s = streams[b.slot];
+        char *base = static_cast<char *>(b.dmem);
+        std::vector<drift_launch> sub(b.pieces.size());
+        for (size_t i = 0; i < b.pieces.size(); i++) {
+            Piece &pc = b.pieces[i];
+            const drift_launch &L = pc.req->L;
             drift_launch &D = sub[i];
             D = L;
-            D.n = p.cn;
-            D.y0 = reinterpret_cast<double *>(base + p.off_y0);
-            cudaMemcpyAsync((void *)D.y0, L.y0 + p.c0 * 6, p.cn * 48, cudaMemcpyHostToDevice, s);
+            D.n = pc.cn;
+            D.y0 = reinterpret_cast<double *>(base + pc.off_y0);
+            cudaMemcpyAsync((void *)D.y0, L.y0 + pc.c0 * 6, pc.cn * 48, cudaMemcpyHostToDevice, s);
             if (L.ts) {
-                D.ts = reinterpret_cast<double *>(base + p.off_grid);
+                D.ts = reinterpret_cast<double *>(base + pc.off_grid);
                 D.t_end = nullptr;
                 cudaMemcpyAsync((void *)D.ts, L.ts, L.nt * sizeof(double), cudaMemcpyHostToDevice, s);
             } else {
-                D.t_end = reinterpret_cast<double *>(base + p.off_grid);
-                cudaMemcpyAsync((void *)D.t_end, L.t_end + p.c0, p.cn * sizeof(double),
+                D.t_end = reinterpret_cast<double *>(base + pc.off_grid);
+                cudaMemcpyAsync((void *)D.t_end, L.t_end + pc.c0, pc.cn * sizeof(double),
                                 cudaMemcpyHostToDevice, s);
             }
-            D.out = L.out ? reinterpret_cast<double *>(base + p.off_out) : nullptr;
-            D.y_final = L.y_final ? reinterpret_cast<double *>(base + p.off_fin) : nullptr;
-            D.status = L.status ? reinterpret_cast<uint8_t *>(base + p.off_st) : nullptr;
-            D.err_code = L.err_code ? reinterpret_cast<int32_t *>(base + p.off_err) : nullptr;
-            D.n_accepted = L.n_accepted ? reinterpret_cast<uint32_t *>(base + p.off_acc) : nullptr;
-            D.n_rejected = L.n_rejected ? reinterpret_cast<uint32_t *>(base + p.off_rej) : nullptr;
-            D.schedule = schedule;
+            D.out = L.out ? reinterpret_cast<double *>(base + pc.off_out) : nullptr;
+            D.y_final = L.y_final ? reinterpret_cast<double *>(base + pc.off_fin) : nullptr;
+            D.status = L.status ? reinterpret_cast<uint8_t *>(base + pc.off_st) : nullptr;
+            D.err_code = L.err_code ? reinterpret_cast<int32_t *>(base + pc.off_err) : nullptr;
+            D.n_accepted = L.n_accepted ? reinterpret_cast<uint32_t *>(base + pc.off_acc) : nullptr;
+            D.n_rejected = L.n_rejected ? reinterpret_cast<uint32_t *>(base + pc.off_rej) : nullptr;
+            D.schedule = b.schedule;
             D.workspace = base;
-            D.workspace_bytes = scratch;
+            D.workspace_bytes = b.scratch;
         }
         drift::TraceRange trace("drift server batch");
-        int rc = drift_internal_launch_batch(launch_sms, sub.data(), (int32_t)sub.size(), base, s);
-        for (size_t i = 0; i < batch->pieces.size(); i++) {
-            Piece &p = batch->pieces[i];
-            const drift_launch &L = p.req->L;
-            const drift_launch &D = sub[i];
-            if (rc != DRIFT_SUCCESS) p.req->result = rc;
-            if (L.out)
-                cudaMemcpy2DAsync(L.out + p.c0 * 6, L.n * 48, D.out, p.cn * 48, p.cn * 48, L.nt,
-                                  cudaMemcpyDeviceToHost, s);
-            if (L.y_final)
-                cudaMemcpyAsync(L.y_final + p.c0 * 6, D.y_final, p.cn * 48, cudaMemcpyDeviceToHost, s);
-            if (L.status) cudaMemcpyAsync(L.status + p.c0, D.status, p.cn, cudaMemcpyDeviceToHost, s);
-            if (L.err_code)
-                cudaMemcpyAsync(L.err_code + p.c0, D.err_code, p.cn * 4, cudaMemcpyDeviceToHost, s);
-            if (L.n_accepted)
-                cudaMemcpyAsync(L.n_accepted + p.c0, D.n_accepted, p.cn * 4, cudaMemcpyDeviceToHost, s);
-            if (L.n_rejected)
-                cudaMemcpyAsync(L.n_rejected + p.c0, D.n_rejected, p.cn * 4, cudaMemcpyDeviceToHost, s);
-            stats.bytes_to_device += p.cn * 48;
-            if (L.out) stats.bytes_to_host += (size_t)L.nt * p.cn * 48;
+        int rc = drift_internal_launch_batch(b.launch_sms, sub.data(), (int32_t)sub.size(), base, s);
+        if (rc == DRIFT_SUCCESS) {
+            for (size_t i = 0; i < b.pieces.size(); i++) {
+                Piece &pc = b.pieces[i];
+                const drift_launch &L = pc.req->L;
+                const drift_launch &D = sub[i];
+                if (L.out)
+                    cudaMemcpy2DAsync(L.out + pc.c0 * 6, L.n * 48, D.out, pc.cn * 48, pc.cn * 48, L.nt,
+                                      cudaMemcpyDeviceToHost, s);
+                if (L.y_final)
+                    cudaMemcpyAsync(L.y_final + pc.c0 * 6, D.y_final, pc.cn * 48, cudaMemcpyDeviceToHost, s);
+                if (L.status) cudaMemcpyAsync(L.status + pc.c0, D.status, pc.cn, cudaMemcpyDeviceToHost, s);
+                if (L.err_code)
+                    cudaMemcpyAsync(L.err_code + pc.c0, D.err_code, pc.cn * 4, cudaMemcpyDeviceToHost, s);
+                if (L.n_accepted)
+                    cudaMemcpyAsync(L.n_accepted + pc.c0, D.n_accepted, pc.cn * 4, cudaMemcpyDeviceToHost, s);
+                if (L.n_rejected)
+                    cudaMemcpyAsync(L.n_rejected + pc.c0, D.n_rejected, pc.cn * 4, cudaMemcpyDeviceToHost, s);
+            }
         }
-        cudaFreeAsync(dmem, s);
-        cudaError_t e = cudaGetLastError();
-        if (e != cudaSuccess)
-            for (Piece &p : batch->pieces) p.req->result = DRIFT_ERROR_CUDA;
-        slot_busy[slot] = true;
-        bytes_inflight += used;
-        stats.batches_launched++;
-        stats.pieces_launched += batch->pieces.size();
-        stats.peak_bytes_in_flight = std::max<uint64_t>(stats.peak_bytes_in_flight, bytes_inflight);
-        Batch *raw = batch.get();
-        inflight.push_back(std::move(batch));
-        auto *ctx = new std::pair<drift_server *, Batch *>(this, raw);
-        if (cudaLaunchHostFunc(s, &drift_server::on_batch_done, ctx) != cudaSuccess) {
-            cudaGetLastError();
-            cudaStreamSynchronize(s);
-            raw->complete = true;
-            delete ctx;
+        cudaFreeAsync(b.dmem, s);
+        cudaError_t e = cudaStreamSynchronize(s);
+        if (e == cudaSuccess) e = cudaGetLastError();
+        else cudaGetLastError();
+        if (rc == DRIFT_SUCCESS && e != cudaSuccess) rc = DRIFT_ERROR_CUDA;
+        return rc;
+    }
+
+    void work(int slot)
+    {
+        cudaSetDevice(device);
+        Worker &w = *workers[slot];
+        std::unique_lock<std::mutex> lock(mu);
+        while (true) {
+            w.cv.wait(lock, [&] { return w.job != nullptr || quit; });
+            if (!w.job) break;  // quit with nothing to do
+            std::unique_ptr<Batch> b = std::move(w.job);
+            lock.unlock();
+            const int rc = execute(*b);
+            lock.lock();
+            for (Piece &pc : b->pieces) {
+                if (rc != DRIFT_SUCCESS) pc.req->result = rc;
+                pc.req->finished += pc.cn;
+                stats.bytes_to_device += pc.cn * 48;
+                if (pc.req->L.out) stats.bytes_to_host += (size_t)pc.req->L.nt * pc.cn * 48;
+                maybe_complete(pc.req);
+            }
+            bytes_inflight -= b->bytes;
+            batches_inflight--;
+            w.busy = false;
+            cv_work.notify_all();
         }
-        return true;
     }
 
     void run()
@@ -352,13 +378,36 @@ struct drift_server {
         cudaSetDevice(device);
         std::unique_lock<std::mutex> lock(mu);
         while (true) {
-            retire();
-            if (stop && inflight.empty()) break;
-            bool progressed = false;
-            if (!stop)
-                while (admit()) progressed = true;
-            if (!progressed)
+            if (stop && batches_inflight == 0) break;
+            std::unique_ptr<Batch> b = stop ? nullptr : plan();
+            if (!b) {
                 cv_work.wait_for(lock, std::chrono::milliseconds(5));
+                continue;
+            }
+            // The allocation is the scheduler's only CUDA call; it runs
+            // without the mutex.  Only this thread plans batches, so the
+            // pieces are still the last particles admitted if they must be
+            // given back.
+            lock.unlock();
+            void *dmem = nullptr;
+            cudaError_t e = cudaMallocFromPoolAsync(&dmem, b->bytes, pool, streams[b->slot]);
+            if (e != cudaSuccess) cudaGetLastError();
+            lock.lock();
+            if (e != cudaSuccess) {
+                give_back(*b);
+                bytes_inflight -= b->bytes;
+                batches_inflight--;
+                workers[b->slot]->busy = false;
+                cv_work.wait_for(lock, std::chrono::milliseconds(5));  // wait for memory
+                continue;
+            }
+            b->dmem = dmem;
+            stats.batches_launched++;
+            stats.pieces_launched += b->pieces.size();
+            stats.peak_bytes_in_flight = std::max<uint64_t>(stats.peak_bytes_in_flight, bytes_inflight);
+            Worker &w = *workers[b->slot];
+            w.job = std::move(b);
+            w.cv.notify_one();
         }
     }
 };
@@ -427,7 +476,6 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
     uint64_t keep = UINT64_MAX;
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     s->streams.resize(o.streams);
-    s->slot_busy.assign(o.streams, false);
     int lowest = 0, greatest = 0;
     cudaDeviceGetStreamPriorityRange(&lowest, &greatest);
     for (size_t i = 0; i < s->streams.size(); i++)
@@ -438,7 +486,10 @@ int drift_server_create(const drift_server_options *options, drift_server **out)
         }
     s->stats.memory_budget = s->budget;
     drift_server *raw = s.release();
-    raw->worker = std::thread([raw] { raw->run(); });
+    for (int i = 0; i < (int)raw->streams.size(); i++) raw->workers.push_back(std::make_unique<drift_server::Worker>());
+    for (int i = 0; i < (int)raw->streams.size(); i++)
+        raw->workers[i]->thread = std::thread([raw, i] { raw->work(i); });
+    raw->scheduler = std::thread([raw] { raw->run(); });
     *out = raw;
     return DRIFT_SUCCESS;
 }
@@ -496,12 +547,29 @@ int drift_server_stats_get(drift_server *s, drift_server_stats *out)
     std::lock_guard<std::mutex> lock(s->mu);
     *out = s->stats;
     out->requests_pending = s->pending.size();
-    out->batches_in_flight = s->inflight.size();
+    out->batches_in_flight = s->batches_inflight;
     out->bytes_in_flight = s->bytes_inflight;
     out->bytes_pending = 0;
     for (const Request *r : s->pending) out->bytes_pending += piece_bytes(r->L, r->L.n - r->admitted);
     out->device = s->device;
     out->reserved = 0;
+    return DRIFT_SUCCESS;
+}
+
+int drift_server_cancel(drift_server *s, uint64_t ticket)
+{
+    if (!s) return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "server is NULL");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->requests.find(ticket);
+    if (it == s->requests.end())
+        return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown ticket");
+    Request *r = it->second.get();
+    if (r->done) return DRIFT_SUCCESS;  // already finished: its result stands
+    r->cancelled = true;
+    auto pos = std::find(s->pending.begin(), s->pending.end(), r);
+    if (pos != s->pending.end()) s->pending.erase(pos);
+    s->maybe_complete(r);  // ends now unless some of its particles are on the GPU
+    s->cv_work.notify_all();
     return DRIFT_SUCCESS;
 }
 
@@ -512,17 +580,21 @@ int drift_server_destroy(drift_server *s)
         std::lock_guard<std::mutex> lock(s->mu);
         s->stop = true;
         for (Request *r : s->pending) {
-            if (r->admitted == 0) {
-                r->result = DRIFT_ERROR_CANCELLED;
-                r->done = true;
-                r->completed = Clock::now();
-            }
+            r->cancelled = true;
+            s->maybe_complete(r);
         }
         s->pending.clear();
         s->cv_done.notify_all();
     }
     s->cv_work.notify_all();
-    if (s->worker.joinable()) s->worker.join();
+    if (s->scheduler.joinable()) s->scheduler.join();  // returns once no batch is in flight
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->quit = true;
+        for (auto &w : s->workers) w->cv.notify_all();
+    }
+    for (auto &w : s->workers)
+        if (w->thread.joinable()) w->thread.join();
     for (auto st : s->streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);

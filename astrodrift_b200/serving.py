@@ -47,6 +47,7 @@ def _lib():
         L.drift_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
         L.drift_server_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+        L.drift_server_cancel.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
         L.drift_server_destroy.argtypes = [ctypes.c_void_p]
         L._server_bound = True
     return L
@@ -76,17 +77,35 @@ class PinnedArray:
             pass
 
 
+class RequestCancelled(RuntimeError):
+    """The request was cancelled before all its particles ran."""
+
+
 class Request:
     def __init__(self, server, ticket, keep, arrays):
         self.server, self.ticket, self._keep, self.arrays = server, ticket, keep, arrays
 
+    def cancel(self) -> None:
+        """Stop admitting this request's particles (drift_server_cancel);
+        wait() then raises RequestCancelled once the particles already on the
+        GPU have finished."""
+        if not self.server._ptr:
+            raise RuntimeError("the server is closed")
+        capi.check(_lib().drift_server_cancel(self.server._ptr, self.ticket), "drift_server_cancel")
+
     def wait(self, timeout: float = 0.0) -> dict:
+        """Block until the request completes; ``timeout`` > 0 bounds the wait
+        (RuntimeError with the library's timeout message when it runs out;
+        the request stays valid and can be waited for again)."""
         if not self.server._ptr:
             raise RuntimeError("the server is closed")
         result = ctypes.c_int(0)
         latency = ctypes.c_double(0.0)
         capi.check(_lib().drift_server_wait(self.server._ptr, self.ticket, timeout, ctypes.byref(result),
                                             ctypes.byref(latency)), "drift_server_wait")
+        if result.value == 7:  # DRIFT_ERROR_CANCELLED
+            self._keep = None
+            raise RequestCancelled("request cancelled")
         if result.value != 0:
             raise RuntimeError(f"request failed: {capi.lib().drift_result_string(result.value).decode()}")
         out = dict(self.arrays)

@@ -449,10 +449,13 @@ int drift_integrate_noalloc(const drift_launch *launch, void *stream);
  * and limits) form one batched launch, and requests larger than the free
  * budget run in particle chunks.  Requests that arrive while others run start
  * as soon as a stream and memory free up; their kernels overlap the running
- * ones.  Trajectory buffers should be page-locked (drift_host_alloc):
- * copies into pageable memory hold the scheduler until they finish.  Results
- * are identical to drift_integrate_host's for the same request.  No
- * counterpart in the reference (which runs one blocking call per stage). */
+ * ones.  Each stream has its own worker thread, and no lock is held across
+ * a CUDA call: a copy into a pageable result buffer (which returns only once
+ * its kernel has finished) holds up only its own stream, never admission,
+ * other streams or the submit/wait/cancel/stats calls.  Page-locked buffers
+ * (drift_host_alloc) still copy faster.  Results are identical to
+ * drift_integrate_host's for the same request.  No counterpart in the
+ * reference (which runs one blocking call per stage). */
 typedef struct drift_server drift_server;
 
 typedef struct {
@@ -491,6 +494,13 @@ int drift_server_submit(drift_server *server, const drift_launch *request, uint6
 int drift_server_wait(drift_server *server, uint64_t ticket, double timeout_s, int *request_result,
                       double *latency_s);
 int drift_server_stats_get(drift_server *server, drift_server_stats *stats);
+/* Cancels one request: none of its particles that are not yet on the GPU
+ * will run.  Particles already admitted finish (their results are written
+ * to the request's buffers), and then the request ends with result
+ * DRIFT_ERROR_CANCELLED, which drift_server_wait reports; a request with
+ * nothing on the GPU ends at once.  Cancelling a request that has already
+ * finished changes nothing.  The ticket stays valid until waited for. */
+int drift_server_cancel(drift_server *server, uint64_t ticket);
 /* Cancels pending requests (their waiters receive DRIFT_ERROR_CANCELLED),
  * finishes the batches in flight and frees the server. */
 int drift_server_destroy(drift_server *server);
