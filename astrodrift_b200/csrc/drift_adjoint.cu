@@ -299,9 +299,9 @@ __device__ __forceinline__ void recompute_step(const Pot &pot, const double *y, 
 template <class Pot, class Jac>
 __global__ void __launch_bounds__(ADJ_THREADS) adjoint_kernel(const __grid_constant__ AdjointArgs a)
 {
-    __shared__ double table[BULGE_TABLE_SIZE];
+    __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
     if (std::is_same<Pot, Bovy>::value) {
-        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
+        stage_bovy_tables(table, a.bulge);
         __syncthreads();
     }
     const Pot pot(a.potential, table);

@@ -89,11 +89,11 @@ __host__ __device__ constexpr bool needs_bulge_table()
 #endif
 
 // Dynamic shared memory per block: the DOP853 rcont parking tile (24
-// doubles per thread, column-major by thread), then the bulge table.
+// doubles per thread, column-major by thread), then the Bovy tables.
 __host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
 {
     return (method == DRIFT_DOP853 ? 24 * sizeof(double) * block : 0) +
-           ((kind == DRIFT_POT_BOVY || kind == DRIFT_POT_MODEL) ? sizeof(BulgeTable) : 0);
+           ((kind == DRIFT_POT_BOVY || kind == DRIFT_POT_MODEL) ? BOVY_SMEM_DOUBLES * sizeof(double) : 0);
 }
 
 // TAPE (DOP853 only): record every accepted step of every particle in
@@ -104,12 +104,12 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
     integrate_kernel(const __grid_constant__ KernelArgs a)
 {
     static_assert(!TAPE || METHOD == DRIFT_DOP853, "the step tape is recorded by DOP853 only");
-    extern __shared__ double smem[];
-    // [park tile (DOP853)][bulge table (Bovy, force models)]
+    extern __shared__ __align__(16) double smem[];
+    // [park tile (DOP853)][Bovy tables (Bovy, force models)]
     volatile double *park = smem + threadIdx.x;
     double *table = smem + (METHOD == DRIFT_DOP853 ? 24 * blockDim.x : 0);
     if (needs_bulge_table<Pot>()) {
-        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
+        stage_bovy_tables(table, a.bulge);
         __syncthreads();
     }
     const Pot pot = make_pot<Pot>(a, table);
@@ -304,10 +304,9 @@ __global__ void __launch_bounds__(256) rank_kernel(const __grid_constant__ Kerne
                                                    uint8_t *keys, unsigned *counts)
 {
     __shared__ unsigned hist[ORDER_BUCKETS];
-    __shared__ double table[BULGE_TABLE_SIZE];
+    __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
     for (int i = threadIdx.x; i < ORDER_BUCKETS; i += blockDim.x) hist[i] = 0;
-    if (needs_bulge_table<Pot>())
-        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = a.bulge.c[i];
+    if (needs_bulge_table<Pot>()) stage_bovy_tables(table, a.bulge);
     __syncthreads();
     const Pot pot = make_pot<Pot>(a, table);
     for (int64_t pid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pid < a.n;
@@ -411,9 +410,9 @@ template <class Pot>
 __global__ void __launch_bounds__(256) force_kernel(drift_potential p, int64_t n, const double *xyz,
                                                     double *acc, const __grid_constant__ BulgeTable bt)
 {
-    __shared__ double table[BULGE_TABLE_SIZE];
+    __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
     if (std::is_same<Pot, Bovy>::value) {
-        for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+        stage_bovy_tables(table, bt);
         __syncthreads();
     }
     const Pot pot(p, table);
@@ -447,8 +446,8 @@ __global__ void __launch_bounds__(256) model_force_kernel(const __grid_constant_
                                                           const __grid_constant__ BulgeTable bt, double t,
                                                           int64_t n, const double *xyz, double *acc)
 {
-    __shared__ double table[BULGE_TABLE_SIZE];
-    for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+    __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
+    stage_bovy_tables(table, bt);
     __syncthreads();
     const Composite pot(&m, table);
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
@@ -469,8 +468,8 @@ __global__ void __launch_bounds__(256) origin_table_kernel(const __grid_constant
                                                            int64_t n_sources, int64_t nt, double t0,
                                                            double dt, const double *traj, double *origins)
 {
-    __shared__ double table[BULGE_TABLE_SIZE];
-    for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) table[i] = bt.c[i];
+    __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
+    stage_bovy_tables(table, bt);
     __syncthreads();
     const Composite pot(&m, table);
     const int64_t total = (nt - 1) * n_sources;

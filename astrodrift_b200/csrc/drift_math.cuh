@@ -26,6 +26,8 @@
 #include <math.h>
 #include <stdint.h>
 
+#include "drift_math_tables.h"
+
 // 1: the translation unit reproduces the reference's rounding (see
 // drift_kernels_exact.cu); 0: multiply-add contraction and a-few-ulp powers.
 #ifndef DRIFT_EXACT_ARITH
@@ -249,6 +251,83 @@ __device__ __forceinline__ double exp_few_ulp(double x)
     p = fma(p, r, 1.0);
     p = fma(p, r, 1.0);
     return p * __longlong_as_double((long long)((int)kd + 1023) << 52);
+}
+
+// ---- table-driven log and exp for the contraction unit's Bovy force ----
+// The tables (drift_math_tables.h, generated with 60-digit arithmetic) are
+// staged in shared memory beside the bulge table; one call reads two (log)
+// or one (exp) entry at a per-lane index.
+//   log x = k ln2 + L_i + log1p(r),  x = 2^k m, m in [1, 2), i = the top 7
+//           bits of m's fraction, r = m * inv_c_i - 1 (one fused multiply-add)
+//           with inv_c_i = RN(1 / (1 + i/128)) and L_i = RN(-ln inv_c_i), so
+//           |r| < 1/128 and log1p(r) needs terms to r^8 (the next one is
+//           below 2^-56 of r).
+//   exp x = 2^e T_j e^r,  x = (64 e + j) ln2 / 64 + r with ln2 / 64 in two
+//           parts, |r| <= ln2 / 128, T_j = RN(2^(j/64)), e^r - 1 to r^5
+//           (the remainder is below 2^-54).
+// exp is within a few ulps for |x| < 708; log within a few ulps for normal
+// x >= 1 and within about 1e-16 absolute below 1 (near 1 from below the
+// k ln2 and L_i terms cancel), which is what its uses need: the halo's
+// ln(1 + u) and the bulge's x^s = exp(s ln x).  Other arguments take the
+// library function out of line.
+constexpr int MATH_TABLE_DOUBLES = 2 * LOG_TABLE_N + EXP_TABLE_N;
+constexpr int MATH_LOG_PAIRS = 0;  // (inv_c_i, L_i) pairs, 16-byte aligned
+constexpr int MATH_EXP_T = 2 * LOG_TABLE_N;
+// ln2 / 64 split so that k * LN2_64_HI is exact for |k| < 2^17
+constexpr double LN2_64_HI = 0x1.62e42fefa0000p-7;
+constexpr double LN2_64_LO = 0x1.cf79abc9e3b3ap-46;
+constexpr double INV_LN2_64 = 0x1.71547652b82fep+6;  // 64 / ln2
+
+// Entry i of the math tables (for the staging loops).
+__device__ __forceinline__ double math_table_entry(int i) { return MATH_TABLE_INIT[i]; }
+
+__device__ __forceinline__ double log_tab(const double *T, double x)
+{
+    if (!(x >= 2.2250738585072014e-308 && x <= 1.7976931348623157e308)) return log_rare(x);
+    const long long bits = __double_as_longlong(x);
+    const int k = (int)(bits >> 52) - 1023;
+    const int i = (int)((bits >> 45) & (LOG_TABLE_N - 1));
+    const double m = __longlong_as_double((bits & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);
+    const double2 e = reinterpret_cast<const double2 *>(T + MATH_LOG_PAIRS)[i];  // (inv_c_i, L_i)
+    const double r = fma(m, e.x, -1.0);
+    double p = -1.0 / 8.0;
+    p = fma(p, r, 1.0 / 7.0);
+    p = fma(p, r, -1.0 / 6.0);
+    p = fma(p, r, 1.0 / 5.0);
+    p = fma(p, r, -1.0 / 4.0);
+    p = fma(p, r, 1.0 / 3.0);
+    p = fma(p, r, -1.0 / 2.0);
+    const double lp = fma(p * r, r, r);  // r + r^2 (-1/2 + r/3 - ...)
+    const double kd = (double)k;
+    return fma(kd, LN2_HI, e.y + fma(kd, LN2_LO, lp));
+}
+
+__device__ __forceinline__ double exp_tab(const double *T, double x)
+{
+    if (!(fabs(x) < 708.0)) return exp_rare(x);
+    const double kd = rint(x * INV_LN2_64);
+    const double r = fma(-kd, LN2_64_LO, fma(-kd, LN2_64_HI, x));
+    const int k = (int)kd;
+    const int j = k & (EXP_TABLE_N - 1);
+    const int e = k >> 6;  // floor(k / 64)
+    double p = 1.0 / 120.0;
+    p = fma(p, r, 1.0 / 24.0);
+    p = fma(p, r, 1.0 / 6.0);
+    p = fma(p, r, 0.5);
+    p = fma(p, r, 1.0) * r;  // e^r - 1
+    const double t = T[MATH_EXP_T + j];
+    return fma(t, p, t) * __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// x^(-1/2) within about an ulp for x in [1e-300, 1e300]: the hardware
+// estimate (rsqrt.approx.ftz.f64, relative error near 2^-23) y0 and, with
+// e = 1 - x y0^2, y = y0 (1 + e/2 + 3 e^2 / 8) (the omitted term is 5 e^3 / 16).
+__device__ __forceinline__ double rsqrt_few_ulp(double x)
+{
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double e = fma(-x * y, y, 1.0);
+    return fma(y * e, fma(0.375, e, 0.5), y);
 }
 
 __device__ __forceinline__ double unit_log(double x)

@@ -11,11 +11,13 @@
 //                   disk :138-151, halo :165-175, bulge = power law with
 //                   exponential cutoff (enclosed-mass force).  In FMA mode
 //                   (DRIFT_EXACT_ARITH 0) the disk and halo use reciprocals
-//                   and rsqrt instead of the reference's divisions.
+//                   and a few-ulp rsqrt instead of the reference's
+//                   divisions, the bulge and halo share one inverse radius,
+//                   and ln / exp come from shared-memory tables.
 // pow(., -1.5) and pow(., 1.5) go through the routines of drift_math.cuh
 // instead of a general pow: correctly rounded in the exact unit, within a
 // few ulps in the contraction unit, which also takes the Bovy force's log
-// and exp from drift_math.cuh's series forms (unit_log, unit_exp).
+// and exp from drift_math.cuh's table forms (log_tab, exp_tab).
 #pragma once
 
 #include "drift_math.cuh"
@@ -116,7 +118,7 @@ struct Plummer {
 // same Horner sum and one power; for x >= 40, gamma = Gamma(s)
 // (Gamma(s, 40) < 1e-15 Gamma(s) for s <= 1.5).
 constexpr int BULGE_PIECES = 20;
-constexpr int BULGE_PIECE_DEG = 17;
+constexpr int BULGE_PIECE_DEG = 17;  // odd: a piece's 18 coefficients load as 9 pairs
 constexpr int BULGE_TABLE_SIZE = BULGE_PIECES * (BULGE_PIECE_DEG + 1);
 constexpr double BULGE_X_CONST = 40.0;
 
@@ -124,18 +126,68 @@ struct BulgeTable {
     double c[BULGE_TABLE_SIZE];
 };
 
-// `table` is the BulgeTable staged in shared memory: each lane reads its own
-// piece, and differing addresses do not serialise there.
+// Shared-memory tables of the Bovy force, staged once per block (16-byte
+// aligned): the bulge table's Taylor pieces, then the contraction unit's log
+// and exp tables (drift_math.cuh).
+constexpr int BOVY_SMEM_DOUBLES = BULGE_TABLE_SIZE + MATH_TABLE_DOUBLES;
+
+__device__ __forceinline__ void stage_bovy_tables(double *smem, const BulgeTable &bt)
+{
+    for (int i = threadIdx.x; i < BULGE_TABLE_SIZE; i += blockDim.x) smem[i] = bt.c[i];
+    for (int i = threadIdx.x; i < MATH_TABLE_DOUBLES; i += blockDim.x)
+        smem[BULGE_TABLE_SIZE + i] = math_table_entry(i);
+}
+
+// x^s from ln and exp: the library functions in the exact unit, the tables
+// (staged after the bulge table) in the contraction unit.
+__device__ __forceinline__ double bulge_power(const double *table, double s, double x)
+{
+#if DRIFT_EXACT_ARITH
+    (void)table;
+    return exp(s * log(x));
+#else
+    const double *T = table + BULGE_TABLE_SIZE;
+    return exp_tab(T, s * log_tab(T, x));
+#endif
+}
+
+// `table` is the Bovy tables staged in shared memory: each lane reads its
+// own piece, and differing addresses do not serialise there.
 __device__ __forceinline__ double bulge_lower_gamma(const double *table, double s, double x, double gamma_s)
 {
     if (x < BULGE_X_CONST) {
         const int j = min((int)(x * 0.5), BULGE_PIECES - 1);
         const double t = x - (2.0 * j + 1.0);
-        const double *c = table + j * (BULGE_PIECE_DEG + 1);
-        double p = c[BULGE_PIECE_DEG];
-#pragma unroll
-        for (int k = BULGE_PIECE_DEG - 1; k >= 0; --k) p = fma(p, t, c[k]);
-        return unit_exp(s * unit_log(x)) * p;
+        // A piece is 18 doubles (144 bytes, 16-byte aligned), read as 9
+        // pairs.  The degree-17 polynomial is evaluated as two halves,
+        // p = P_lo(t) + t^9 P_hi(t) with P_lo = c0..c8 and P_hi = c9..c17,
+        // whose Horner chains (8 multiply-adds each) run side by side: half
+        // the dependent latency of one 17-term chain for four extra
+        // multiplications.
+        static_assert(BULGE_PIECE_DEG == 17, "the split below assumes 18 coefficients");
+        const double2 *c = reinterpret_cast<const double2 *>(table + j * (BULGE_PIECE_DEG + 1));
+        const double2 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3], c4 = c[4], c5 = c[5], c6 = c[6],
+                      c7 = c[7], c8 = c[8];
+        // P_lo: c0 .. c8 = c0.x c0.y c1.x c1.y c2.x c2.y c3.x c3.y c4.x
+        double lo = fma(c4.x, t, c3.y);
+        lo = fma(lo, t, c3.x);
+        lo = fma(lo, t, c2.y);
+        lo = fma(lo, t, c2.x);
+        lo = fma(lo, t, c1.y);
+        lo = fma(lo, t, c1.x);
+        lo = fma(lo, t, c0.y);
+        lo = fma(lo, t, c0.x);
+        // P_hi: c9 .. c17 = c4.y c5.x c5.y c6.x c6.y c7.x c7.y c8.x c8.y
+        double hi = fma(c8.y, t, c8.x);
+        hi = fma(hi, t, c7.y);
+        hi = fma(hi, t, c7.x);
+        hi = fma(hi, t, c6.y);
+        hi = fma(hi, t, c6.x);
+        hi = fma(hi, t, c5.y);
+        hi = fma(hi, t, c5.x);
+        hi = fma(hi, t, c4.y);
+        const double t2 = t * t, t4 = t2 * t2, t9 = (t4 * t4) * t;
+        return bulge_power(table, s, x) * fma(hi, t9, lo);
     }
     return gamma_s;
 }
@@ -157,19 +209,14 @@ struct Bovy {
     __device__ DRIFT_FORCE_FN void force(double x, double y, double z, double &ax, double &ay,
                                           double &az) const
     {
+#if DRIFT_EXACT_ARITH
         // bulge
         double bx = 0.0, by = 0.0, bz = 0.0;
         double r2s = x * x + y * y + z * z;
         if (r2s != 0.0) {
-#if DRIFT_EXACT_ARITH
             double r = sqrt(r2s);
             double g = bulge_lower_gamma(table, bulge_s, r2s / bulge_rc2, bulge_gamma_s);
             double ar_over_r = -bulge_k * g / (r2s * r);
-#else
-            double inv_r = rsqrt(r2s);
-            double g = bulge_lower_gamma(table, bulge_s, r2s * inv_rc2, bulge_gamma_s);
-            double ar_over_r = -bulge_k * g * (inv_r * inv_r * inv_r);
-#endif
             bx = ar_over_r * x;
             by = ar_over_r * y;
             bz = ar_over_r * z;
@@ -179,7 +226,6 @@ struct Bovy {
         {
             double r2 = x * x + y * y;
             double z2 = z * z;
-#if DRIFT_EXACT_ARITH
             double r = sqrt(r2);
             double sqrtz2b2 = sqrt(z2 + mn_b2);
             double apz = mn_a + sqrtz2b2;
@@ -189,37 +235,56 @@ struct Bovy {
             dx = ar * (x / r);
             dy = ar * (y / r);
             dz = -mn_amp * (z * apz) / (sqrtz2b2 * denom);
-#else
-            // a_R x/R == -amp x / D with D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
-            double inv_sz = rsqrt(z2 + mn_b2);
-            double apz = fma(z2 + mn_b2, inv_sz, mn_a);
-            double m_over_d = -mn_amp * unit_pow_m1p5(fma(apz, apz, r2));
-            dx = m_over_d * x;
-            dy = m_over_d * y;
-            dz = m_over_d * z * apz * inv_sz;
-#endif
         }
         // NFW halo
         double hx, hy, hz;
         {
             double r2 = r2s;
-#if DRIFT_EXACT_ARITH
             double r = sqrt(r2);
             double ar = -nfw_amp * (log(1. + r / nfw_a) - r / (nfw_a + r)) / r2;
             hx = ar * (x / r);
             hy = ar * (y / r);
             hz = ar * (z / r);
+        }
 #else
-            double inv_r = rsqrt(r2);
-            double r = r2 * inv_r;
-            double u = r * inv_nfw_a;
-            double term = unit_log(1. + u) - u * fast_rcp(1.0 + u);
-            double ar_over_r = -nfw_amp * term * (inv_r * inv_r * inv_r);
+        // One inverse radius serves the bulge and the halo.
+        const double r2s = x * x + y * y + z * z;
+        const double inv_r = rsqrt_few_ulp(r2s);
+        const double inv_r3 = inv_r * inv_r * inv_r;
+        // bulge
+        double bx = 0.0, by = 0.0, bz = 0.0;
+        if (r2s != 0.0) {
+            const double g = bulge_lower_gamma(table, bulge_s, r2s * inv_rc2, bulge_gamma_s);
+            const double ar_over_r = -bulge_k * g * inv_r3;
+            bx = ar_over_r * x;
+            by = ar_over_r * y;
+            bz = ar_over_r * z;
+        }
+        // Miyamoto-Nagai disk: a_R x/R == -amp x / D with
+        // D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
+        double dx, dy, dz;
+        {
+            const double r2 = x * x + y * y;
+            const double zb2 = z * z + mn_b2;
+            const double inv_sz = rsqrt_few_ulp(zb2);
+            const double apz = fma(zb2, inv_sz, mn_a);
+            const double m_over_d = -mn_amp * unit_pow_m1p5(fma(apz, apz, r2));
+            dx = m_over_d * x;
+            dy = m_over_d * y;
+            dz = m_over_d * z * apz * inv_sz;
+        }
+        // NFW halo
+        double hx, hy, hz;
+        {
+            const double r = r2s * inv_r;
+            const double u = r * inv_nfw_a;
+            const double term = log_tab(table + BULGE_TABLE_SIZE, 1. + u) - u * fast_rcp(1.0 + u);
+            const double ar_over_r = -nfw_amp * term * inv_r3;
             hx = ar_over_r * x;
             hy = ar_over_r * y;
             hz = ar_over_r * z;
-#endif
         }
+#endif
         ax = (bx + dx) + hx;
         ay = (by + dy) + hy;
         az = (bz + dz) + hz;
