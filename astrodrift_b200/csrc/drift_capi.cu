@@ -15,6 +15,8 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <chrono>
+#include <thread>
 #include <vector>
 
 #include "drift_b200.h"
@@ -116,6 +118,7 @@ struct DeviceContext {
     DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor, origins;
     DevBuf src_traj, src_table, src_origins;  // drift_origin_table_host
     HostBuf stage[2];
+    HostBuf poll;  // streamed copy-out: the chunk completion counters, read back
 
     DevBuf *dev_bufs[14] = {&y0, &grid, &out[0], &out[1], &yfin, &status, &err, &acc, &rej, &cursor,
                             &origins, &src_traj, &src_table, &src_origins};
@@ -128,13 +131,14 @@ struct DeviceContext {
         for (const DevBuf *d : dev_bufs) b += d->bytes;
         return b;
     }
-    size_t pinned_bytes() const { return stage[0].bytes + stage[1].bytes; }
+    size_t pinned_bytes() const { return stage[0].bytes + stage[1].bytes + poll.bytes; }
     // Waits for the streams and frees every buffer, stream and event (device current).
     void release()
     {
         for (int i = 0; i < 2; i++)
             if (streams[i]) cudaStreamSynchronize(streams[i]);
         for (DevBuf *d : dev_bufs) d->release();
+        poll.release();
         for (int i = 0; i < 2; i++) {
             stage[i].release();
             if (done[i]) cudaEventDestroy(done[i]);
@@ -828,6 +832,160 @@ int drift_host_free(void *ptr)
 
 static int host_integrate(DeviceContext *ctx, const drift_launch *L);
 
+// Requests above this many particles may take the streamed copy-out.
+constexpr int64_t STREAMED_MIN_PARTICLES = 65536;
+// Particle chunks of a streamed copy-out.
+constexpr int STREAMED_CHUNKS = 32;
+
+static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
+
+// The streamed copy-out of drift_integrate_host (the request's trajectory
+// destination is page-locked and fits the device whole).  One launch
+// integrates every particle into a full (nt, n, 6) device array; its queue
+// (drift::build_order_chunked) runs the particles that outlast a chunk's
+// share of the launch first, then chunk 0's particles longest first, then
+// chunk 1's, and so on, and every particle counts itself done in its chunk's
+// counter.  This thread reads the counters back every 200 microseconds (a
+// small copy on the second stream) and copies each finished chunk's
+// trajectory to the caller as soon as its counter is full, so the copy-out
+// overlaps the rest of the launch and only the last chunks' copies remain
+// after it.  The loop ends when every chunk is copied; once the launch's
+// completion event fires, whatever is left is copied at once, so a launch
+// that ends early (an error, a timeout) never leaves the loop waiting.
+static int stream_copy_out(DeviceContext *ctx, const drift_launch *L)
+{
+    drift::TraceRange trace("drift host streamed copy-out");
+    const int64_t n = L->n;
+    const int64_t nt = L->nt;
+    const size_t row = 6 * sizeof(double);
+    cudaStream_t s0 = ctx->streams[0], s1 = ctx->streams[1];
+
+    const int64_t chunk_len = ((n + STREAMED_CHUNKS - 1) / STREAMED_CHUNKS + 127) / 128 * 128;
+    const int nchunks = (int)((n + chunk_len - 1) / chunk_len);
+    const size_t scratch = drift::chunked_order_scratch(nchunks);
+    const size_t ws = CURSOR_BYTES + scratch + align256(nchunks * sizeof(unsigned)) + align256(4 * (size_t)n) +
+                      align256((size_t)n);
+    DRIFT_CUDA_TRY(ctx->out[0].ensure((size_t)nt * n * row), "cudaMalloc(trajectory)");
+    DRIFT_CUDA_TRY(ctx->cursor.ensure(ws), "cudaMalloc(workspace)");
+    DRIFT_CUDA_TRY(ctx->poll.ensure(nchunks * sizeof(unsigned)), "cudaMallocHost(chunk counters)");
+
+    // inputs
+    drift_force_model model_dev{};
+    drift_launch sub = *L;
+    if (L->potential.kind == DRIFT_POT_MODEL) {
+        model_dev = *L->force_model;
+        if (model_dev.n_groups > 0) {
+            const size_t bytes = (size_t)model_dev.n_segments * model_dev.n_sources * 18 * sizeof(double);
+            DRIFT_CUDA_TRY(ctx->origins.ensure(bytes), "cudaMalloc(origins)");
+            DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->origins.ptr, model_dev.origins, bytes, cudaMemcpyHostToDevice, s0),
+                           "H2D origins");
+            model_dev.origins = ctx->origins.as<double>();
+        }
+        sub.force_model = &model_dev;
+    }
+    const bool columns = L->y0_layout == DRIFT_Y0_COLUMNS;
+    if (columns) {
+        const size_t spitch = (size_t)(L->y0_stride ? L->y0_stride : n) * sizeof(double);
+        DRIFT_CUDA_TRY(cudaMemcpy2DAsync(ctx->y0.ptr, n * sizeof(double), L->y0, spitch, n * sizeof(double), 6,
+                                         cudaMemcpyHostToDevice, s0),
+                       "H2D y0 columns");
+    } else {
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->y0.ptr, L->y0, n * row, cudaMemcpyHostToDevice, s0), "H2D y0");
+    }
+    const size_t grid_bytes = L->ts ? nt * sizeof(double) : n * sizeof(double);
+    DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->grid.ptr, L->ts ? (const void *)L->ts : (const void *)L->t_end,
+                                   grid_bytes, cudaMemcpyHostToDevice, s0),
+                   "H2D grid");
+    sub.y0 = ctx->y0.as<double>();
+    sub.y0_stride = columns ? n : 0;
+    sub.ts = L->ts ? ctx->grid.as<double>() : nullptr;
+    sub.t_end = L->ts ? nullptr : ctx->grid.as<double>();
+    sub.out = ctx->out[0].as<double>();
+    sub.y_final = L->y_final ? ctx->yfin.as<double>() : nullptr;
+    sub.status = L->status ? ctx->status.as<uint8_t>() : nullptr;
+    sub.err_code = L->err_code ? ctx->err.as<int32_t>() : nullptr;
+    sub.n_accepted = L->n_accepted ? ctx->acc.as<uint32_t>() : nullptr;
+    sub.n_rejected = L->n_rejected ? ctx->rej.as<uint32_t>() : nullptr;
+    sub.schedule = DRIFT_SCHEDULE_ORDERED;
+
+    // the chunk-ordered queue and the launch, on stream 0
+    char *base = static_cast<char *>(ctx->cursor.ptr);
+    unsigned *counts = reinterpret_cast<unsigned *>(base + CURSOR_BYTES);
+    unsigned *split = counts + 256;
+    unsigned *chunk_counts = split + 1;
+    unsigned *done = reinterpret_cast<unsigned *>(base + CURSOR_BYTES + scratch);
+    uint32_t *order = reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(done) + align256(nchunks * sizeof(unsigned)));
+    uint8_t *keys = reinterpret_cast<uint8_t *>(order) + align256(4 * (size_t)n);
+    drift::KernelArgs a = make_args(&sub);
+    const int block = block_of(&sub);
+    int grid = 0;
+    int rc = grid_for(ctx->sm_count, &sub, n, block, &grid);
+    if (rc) return rc;
+    a.persistent = 1;
+    a.cursor = reinterpret_cast<unsigned long long *>(base);
+    a.chunk_done = done;
+    a.chunk_len = chunk_len;
+    DRIFT_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(unsigned long long), s0), "cudaMemsetAsync");
+    DRIFT_CUDA_TRY(cudaMemsetAsync(done, 0, nchunks * sizeof(unsigned), s0), "cudaMemsetAsync");
+    // stream 1 reads the counters only after they are cleared
+    DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[1], s0), "cudaEventRecord");
+    DRIFT_CUDA_TRY(cudaStreamWaitEvent(s1, ctx->done[1], 0), "cudaStreamWaitEvent");
+    DRIFT_CUDA_TRY(drift::build_order_chunked(a, sub.method, keys, counts, split, chunk_counts, order, chunk_len,
+                                              nchunks, (int64_t)grid * block, ctx->sm_count, s0),
+                   "ordering kernels");
+    a.order = order;
+    DRIFT_CUDA_TRY(launch_args(a, sub.method, sub.precision, grid, block, s0), "kernel launch");
+    DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[0], s0), "cudaEventRecord");
+
+    // copy-out as chunks complete, on stream 1
+    const unsigned *seen = static_cast<const unsigned *>(ctx->poll.ptr);
+    std::vector<char> copied(nchunks, 0);
+    int remaining = nchunks;
+    while (remaining > 0) {
+        const cudaError_t q = cudaEventQuery(ctx->done[0]);
+        if (q != cudaSuccess && q != cudaErrorNotReady) return cuda_fail(q, "integration launch");
+        const bool launch_done = q == cudaSuccess;
+        if (launch_done) {
+            DRIFT_CUDA_TRY(cudaStreamWaitEvent(s1, ctx->done[0], 0), "cudaStreamWaitEvent");
+        } else {
+            cudaGetLastError();  // clears the not-ready status
+            DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->poll.ptr, done, nchunks * sizeof(unsigned), cudaMemcpyDeviceToHost, s1),
+                           "D2H chunk counters");
+            DRIFT_CUDA_TRY(cudaStreamSynchronize(s1), "cudaStreamSynchronize");
+        }
+        for (int c = 0; c < nchunks; c++) {
+            if (copied[c]) continue;
+            const int64_t c0 = (int64_t)c * chunk_len;
+            const int64_t cn = std::min(chunk_len, n - c0);
+            if (!launch_done && (int64_t)seen[c] < cn) continue;
+            DRIFT_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<char *>(L->out) + c0 * row, n * row,
+                                             sub.out + c0 * 6, n * row, cn * row, nt, cudaMemcpyDeviceToHost, s1),
+                           "D2H trajectory chunk");
+            copied[c] = 1;
+            remaining--;
+        }
+        if (remaining > 0) std::this_thread::sleep_for(std::chrono::microseconds(200));
+    }
+
+    // per-particle outputs once the launch is done
+    if (L->y_final)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->y_final, ctx->yfin.ptr, n * row, cudaMemcpyDeviceToHost, s0), "D2H y_final");
+    if (L->status)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->status, ctx->status.ptr, n, cudaMemcpyDeviceToHost, s0), "D2H status");
+    if (L->err_code)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->err_code, ctx->err.ptr, n * sizeof(int32_t), cudaMemcpyDeviceToHost, s0),
+                       "D2H err");
+    if (L->n_accepted)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->n_accepted, ctx->acc.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s0),
+                       "D2H accepted");
+    if (L->n_rejected)
+        DRIFT_CUDA_TRY(cudaMemcpyAsync(L->n_rejected, ctx->rej.ptr, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, s0),
+                       "D2H rejected");
+    DRIFT_CUDA_TRY(cudaStreamSynchronize(s0), "cudaStreamSynchronize");
+    DRIFT_CUDA_TRY(cudaStreamSynchronize(s1), "cudaStreamSynchronize");
+    return DRIFT_SUCCESS;
+}
+
 extern "C" {
 
 int drift_integrate_host(const drift_launch *L)
@@ -864,12 +1022,22 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
     if (L->n_rejected) DRIFT_CUDA_TRY(ctx->rej.ensure(n * sizeof(uint32_t)), "cudaMalloc(rej)");
     // (the per-slot workspace is sized once the chunk length is known)
 
-    // Trajectory chunks: particles [c0, c0 + cn) write a (nt, cn, 6) device
-    // block that is copied out row by row into the caller's (nt, n, 6) array.
+    // Streamed copy-out (large persistent or ordered requests into page-locked
+    // memory whose whole trajectory fits the device): one launch over every
+    // particle with a queue that completes particle chunks in order, each
+    // chunk copied out as soon as it is done (stream_copy_out below).
+    // Otherwise, trajectory chunks: particles [c0, c0 + cn) write a
+    // (nt, cn, 6) device block that is copied out row by row into the
+    // caller's (nt, n, 6) array while the next chunk integrates.
+    const bool out_pinned = L->out && is_pinned(L->out);
+    size_t free_b = 0, total_b = 0;
+    if (L->out) DRIFT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    const size_t out_bytes = L->out ? (size_t)nt * n * row : 0;
+    const bool streamed = out_pinned && L->schedule != DRIFT_SCHEDULE_PLAIN && n > STREAMED_MIN_PARTICLES &&
+                          out_bytes <= (free_b + ctx->out[0].bytes) / 10 * 6;
+    if (streamed) return stream_copy_out(ctx, L);
     int64_t chunk = n;
     if (L->out) {
-        size_t free_b = 0, total_b = 0;
-        DRIFT_CUDA_TRY(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
         const size_t budget = std::min<size_t>(free_b / 4, size_t(8) << 30);
         int64_t by_mem = (int64_t)(budget / (nt * row));
         // Several chunks when the output is large, so the device->host copy
@@ -888,7 +1056,6 @@ static int host_integrate(DeviceContext *ctx, const drift_launch *L)
     chunk_req.n = chunk;
     const size_t ws_slot = std::max<size_t>(workspace_bytes(&chunk_req), CURSOR_BYTES);
     DRIFT_CUDA_TRY(ctx->cursor.ensure(2 * ws_slot), "cudaMalloc(workspace)");
-    const bool out_pinned = L->out && is_pinned(L->out);
     if (L->out && !out_pinned)
         for (int i = 0; i < 2; i++)
             DRIFT_CUDA_TRY(ctx->stage[i].ensure(chunk * nt * row), "cudaMallocHost(stage)");

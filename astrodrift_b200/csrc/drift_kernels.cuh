@@ -79,14 +79,32 @@ __host__ __device__ constexpr bool needs_bulge_table()
 
 
 // Launch bounds of the integration kernels: at most DRIFT_MAX_THREADS
-// threads per block, and registers allocated so that DRIFT_MIN_BLOCKS_PER_SM
-// such blocks can be resident on one SM.
+// threads per block, and registers allocated so that a given number of such
+// blocks can be resident on one SM.  Registers are allocated per scheduler
+// (16K each), so the choices are two warps per scheduler (up to 255
+// registers), three (168) or four (128).
+//   DOP853: DRIFT_MIN_BLOCKS_DOP853 = 2 blocks of 128.  Its step needs about
+//     250 registers; with them and no spills two warps per scheduler beat
+//     three warps that spill: the uneven Bovy workload's 2^18-particle slice
+//     0.87 s against 1.18 s per pass (4 blocks: 1.55 s), the Plummer workload
+//     70.8 against 71.7 ms.
+//   DOPR54: DRIFT_MIN_BLOCKS_PER_SM = 3 (the Kepler configuration: 7.15 ms
+//     against 7.22 ms at 2).
 #ifndef DRIFT_MAX_THREADS
 #define DRIFT_MAX_THREADS 128
 #endif
 #ifndef DRIFT_MIN_BLOCKS_PER_SM
 #define DRIFT_MIN_BLOCKS_PER_SM 3
 #endif
+#ifndef DRIFT_MIN_BLOCKS_DOP853
+#define DRIFT_MIN_BLOCKS_DOP853 2
+#endif
+
+template <int METHOD, class Pot>
+struct LaunchShape {
+    static constexpr int threads = DRIFT_MAX_THREADS;
+    static constexpr int min_blocks = METHOD == DRIFT_DOP853 ? DRIFT_MIN_BLOCKS_DOP853 : DRIFT_MIN_BLOCKS_PER_SM;
+};
 
 // Dynamic shared memory per block: the DOP853 rcont parking tile (24
 // doubles per thread, column-major by thread), then the Bovy tables.
@@ -100,7 +118,7 @@ __host__ __device__ constexpr size_t smem_bytes(int method, int kind, int block)
 // a.tape for the adjoint pass; a particle whose tape is full stops with
 // DRIFT_PARTICLE_TAPE_FULL.
 template <int METHOD, class Pot, bool TAPE = false>
-__global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
+__global__ void __launch_bounds__(LaunchShape<METHOD, Pot>::threads, LaunchShape<METHOD, Pot>::min_blocks)
     integrate_kernel(const __grid_constant__ KernelArgs a)
 {
     static_assert(!TAPE || METHOD == DRIFT_DOP853, "the step tape is recorded by DOP853 only");
@@ -211,6 +229,11 @@ __global__ void __launch_bounds__(DRIFT_MAX_THREADS, DRIFT_MIN_BLOCKS_PER_SM)
         if (ec) ec[pid] = code;
         if (na) na[pid] = nacc;
         if (nr) nr[pid] = nrej;
+        if (a.chunk_done) {
+            // every write of this particle is visible before it counts as done
+            __threadfence();
+            atomicAdd(a.chunk_done + pid / a.chunk_len, 1u);
+        }
         active = false;
     };
 
@@ -383,6 +406,130 @@ __global__ void __launch_bounds__(256) order_scatter_kernel(int64_t n, const uin
             order[pos + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)pid;
         }
     }
+}
+
+// ---- chunk-ordered queue (streamed copy-out) -----------------------------
+//
+// Bucket b of the rank histogram holds particles of cost about
+// 2^((127.5 - b) / 4) (key = 255 - b = floor(4 log2 cost) + 128).  One
+// thread finds the first bucket whose cost is below total / (lanes x
+// nchunks): particles in buckets before it last longer than a chunk's share
+// of the launch and go first; the rest are queued chunk by chunk.
+__global__ void __launch_bounds__(32) chunk_split_kernel(const unsigned *counts, double lanes_x_chunks,
+                                                         unsigned *split)
+{
+    if (threadIdx.x != 0) return;
+    double total = 0.0;
+    for (int b = 0; b < ORDER_BUCKETS; b++) total += (double)counts[b] * exp2((127.5 - b) * 0.25);
+    const double threshold = total / lanes_x_chunks;
+    unsigned k = ORDER_BUCKETS;
+    for (int b = 0; b < ORDER_BUCKETS; b++)
+        if (exp2((127.5 - b) * 0.25) < threshold) {
+            k = b;
+            break;
+        }
+    *split = k;
+}
+
+__device__ __forceinline__ int chunk_bucket(int64_t pid, const uint8_t *keys, int64_t chunk_len, unsigned split)
+{
+    const int b = ORDER_BUCKETS - 1 - keys[pid];
+    const int cls = (unsigned)b < split ? 0 : 1 + (int)(pid / chunk_len);
+    return cls * ORDER_BUCKETS + b;
+}
+
+__global__ void __launch_bounds__(256) chunk_hist_kernel(int64_t n, const uint8_t *keys, int64_t chunk_len,
+                                                         const unsigned *split, unsigned *chunk_counts)
+{
+    const unsigned k = *split;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = base + threadIdx.x;
+        const bool valid = pid < n;
+        const int id = valid ? chunk_bucket(pid, keys, chunk_len, k) : -1 - (int)(threadIdx.x & 31);
+        const unsigned peers = __match_any_sync(0xffffffffu, id);
+        if (valid && (threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&chunk_counts[id], (unsigned)__popc(peers));
+    }
+}
+
+// Exclusive prefix sum of `count` entries in place (one block of 1024).
+__global__ void __launch_bounds__(1024) chunk_scan_kernel(unsigned *v, int count)
+{
+    __shared__ unsigned tile[1024];
+    __shared__ unsigned carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < count; base += 1024) {
+        const int i = base + threadIdx.x;
+        const unsigned x = i < count ? v[i] : 0u;
+        tile[threadIdx.x] = x;
+        __syncthreads();
+        for (int off = 1; off < 1024; off <<= 1) {
+            const unsigned add = threadIdx.x >= off ? tile[threadIdx.x - off] : 0u;
+            __syncthreads();
+            tile[threadIdx.x] += add;
+            __syncthreads();
+        }
+        if (i < count) v[i] = carry + tile[threadIdx.x] - x;
+        __syncthreads();
+        if (threadIdx.x == 1023) carry += tile[1023];
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256) chunk_scatter_kernel(int64_t n, const uint8_t *keys, int64_t chunk_len,
+                                                            const unsigned *split, unsigned *offsets,
+                                                            uint32_t *order)
+{
+    const unsigned k = *split;
+    for (int64_t base = (int64_t)blockIdx.x * blockDim.x; base < n; base += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t pid = base + threadIdx.x;
+        const bool valid = pid < n;
+        const int id = valid ? chunk_bucket(pid, keys, chunk_len, k) : -1 - (int)(threadIdx.x & 31);
+        const unsigned peers = __match_any_sync(0xffffffffu, id);
+        if (valid) {
+            const int lane = threadIdx.x & 31;
+            const int leader = __ffs(peers) - 1;
+            unsigned pos = 0;
+            if (lane == leader) pos = atomicAdd(&offsets[id], (unsigned)__popc(peers));
+            pos = __shfl_sync(peers, pos, leader);
+            order[pos + __popc(peers & ((1u << lane) - 1u))] = (uint32_t)pid;
+        }
+    }
+}
+
+inline cudaError_t launch_rank(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts, int grid,
+                               cudaStream_t stream)
+{
+    switch (a.potential.kind) {
+    case DRIFT_POT_KEPLER: rank_kernel<KeplerGalpy><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_PLUMMER: rank_kernel<Plummer><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_BOVY: rank_kernel<Bovy><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    case DRIFT_POT_KEPLER_CARTESIAN:
+        rank_kernel<KeplerCartesian><<<grid, 256, 0, stream>>>(a, method, keys, counts);
+        break;
+    case DRIFT_POT_MODEL: rank_kernel<Composite><<<grid, 256, 0, stream>>>(a, method, keys, counts); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+inline cudaError_t build_order_chunked_impl(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                                            unsigned *split, unsigned *chunk_counts, uint32_t *order,
+                                            int64_t chunk_len, int nchunks, int64_t lanes, int sm_count,
+                                            cudaStream_t stream)
+{
+    const int entries = (nchunks + 1) * ORDER_BUCKETS;
+    cudaError_t e = cudaMemsetAsync(counts, 0, ORDER_BUCKETS * sizeof(unsigned), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(chunk_counts, 0, entries * sizeof(unsigned), stream);
+    if (e != cudaSuccess) return e;
+    const int grid = (int)std::min<int64_t>((a.n + 255) / 256, (int64_t)sm_count * 8);
+    e = launch_rank(a, method, keys, counts, grid, stream);
+    if (e != cudaSuccess) return e;
+    chunk_split_kernel<<<1, 32, 0, stream>>>(counts, (double)lanes * nchunks, split);
+    chunk_hist_kernel<<<grid, 256, 0, stream>>>(a.n, keys, chunk_len, split, chunk_counts);
+    chunk_scan_kernel<<<1, 1024, 0, stream>>>(chunk_counts, entries);
+    chunk_scatter_kernel<<<grid, 256, 0, stream>>>(a.n, keys, chunk_len, split, chunk_counts, order);
+    return cudaGetLastError();
 }
 
 inline cudaError_t build_order_impl(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,

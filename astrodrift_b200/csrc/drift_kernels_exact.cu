@@ -37,6 +37,13 @@ cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned
 {
     return exact::build_order_impl(a, method, keys, counts, order, sm_count, stream);
 }
+cudaError_t build_order_chunked(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                                unsigned *split, unsigned *chunk_counts, uint32_t *order, int64_t chunk_len,
+                                int nchunks, int64_t lanes, int sm_count, cudaStream_t stream)
+{
+    return exact::build_order_chunked_impl(a, method, keys, counts, split, chunk_counts, order, chunk_len, nchunks,
+                                           lanes, sm_count, stream);
+}
 cudaError_t occupancy_exact(int method, int kind, int block, bool tape, int *blocks_per_sm)
 {
     return exact::occupancy_impl(method, kind, block, tape, blocks_per_sm);

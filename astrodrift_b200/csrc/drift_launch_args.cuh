@@ -70,6 +70,10 @@ struct KernelArgs {
     int32_t arbitrary_times;     // DOPR54: intervals end at ts[i + 1]
     int32_t tape_stride;         // step tape layout (see drift_launch.tape_stride)
     int32_t sparse_output;       // every grid has <= SPARSE_OUTPUT_NT times (see Dop853Lane::step)
+    // Streamed copy-out (host path): particle p, once finished, counts itself
+    // in chunk_done[p / chunk_len]; NULL = no counting.
+    unsigned *chunk_done;
+    int64_t chunk_len;
     drift_potential potential;
     BulgeTable bulge;            // Bovy (or a force model with Bovy parts): incomplete gamma table
     drift_force_model model;     // potential.kind == DRIFT_POT_MODEL: the summed force
@@ -92,6 +96,21 @@ int max_threads_fma();
 // `keys` n bytes of scratch.
 cudaError_t build_order(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
                         uint32_t *order, int sm_count, cudaStream_t stream);
+// Longest-first queue for a streamed launch whose particles are copied out
+// chunk by chunk: particles too long to finish within one chunk's share of
+// the launch go first (longest first), then chunk 0's particles longest
+// first, then chunk 1's, and so on, so that the chunks complete in order.
+// Scratch: counts 256 + split 1 + chunk_counts (nchunks + 1) * 256 uint32,
+// keys n bytes.  `lanes` is the launch's resident thread count.
+cudaError_t build_order_chunked(const KernelArgs &a, int method, uint8_t *keys, unsigned *counts,
+                                unsigned *split, unsigned *chunk_counts, uint32_t *order, int64_t chunk_len,
+                                int nchunks, int64_t lanes, int sm_count, cudaStream_t stream);
+// Scratch bytes build_order_chunked needs beside the queue (counts, split
+// and chunk counts, 256-byte aligned).
+inline size_t chunked_order_scratch(int nchunks)
+{
+    return ((256 + 1 + (size_t)(nchunks + 1) * 256) * sizeof(unsigned) + 255) / 256 * 256;
+}
 cudaError_t force_exact(const drift_potential &p, int64_t n, const double *xyz, double *acc,
                         const BulgeTable &bt, int grid, cudaStream_t stream);
 cudaError_t force_fma(const drift_potential &p, int64_t n, const double *xyz, double *acc,
