@@ -32,12 +32,24 @@ struct Grid {
     }
 };
 
+// 1: trajectory samples are written with streaming (evict-first) stores;
+// 0: with ordinary write-back stores.
+#ifndef DRIFT_STREAMING_STORES
+#define DRIFT_STREAMING_STORES 1
+#endif
+
 __device__ __forceinline__ void store6(double *dst, const double *v)
 {
     double2 *p = reinterpret_cast<double2 *>(dst);
+#if DRIFT_STREAMING_STORES
     __stcs(p + 0, make_double2(v[0], v[1]));
     __stcs(p + 1, make_double2(v[2], v[3]));
     __stcs(p + 2, make_double2(v[4], v[5]));
+#else
+    p[0] = make_double2(v[0], v[1]);
+    p[1] = make_double2(v[2], v[3]);
+    p[2] = make_double2(v[4], v[5]);
+#endif
 }
 
 // Writes one 6-vector of particle `pid` at output slot k of a time-major

@@ -30,6 +30,12 @@
 #define DRIFT_EXACT_ARITH 1
 #endif
 
+// 1: the eight-term partial sums of rcont5..8 wait out the three extra
+// stages in shared memory (the `park` tile); 0: in registers.
+#ifndef DRIFT_PARK_RCONT
+#define DRIFT_PARK_RCONT 1
+#endif
+
 namespace drift {
 namespace dop853c {
 constexpr double UROUND = 2.3e-16;
@@ -413,19 +419,25 @@ struct Dop853Lane {
             const bool skip_dense =
                 sparse_output && !(next < grid.nt - 1 && pos_neg * grid.at(next + 1) < pos_neg * t_new);
             if (!skip_dense) {
+#if DRIFT_PARK_RCONT
+#define DRIFT_PARKED(j, i) park[((j) * 6 + (i)) * RCONT_STRIDE]
+#else
+                double parked[24];
+#define DRIFT_PARKED(j, i) parked[(j) * 6 + (i)]
+#endif
 
 #pragma unroll
                 for (int i = 0; i < 6; i++) {
-                    park[(0 * 6 + i) * RCONT_STRIDE] =
+                    DRIFT_PARKED(0, i) =
                         D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
                         D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
-                    park[(1 * 6 + i) * RCONT_STRIDE] =
+                    DRIFT_PARKED(1, i) =
                         D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
                         D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
-                    park[(2 * 6 + i) * RCONT_STRIDE] =
+                    DRIFT_PARKED(2, i) =
                         D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
                         D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
-                    park[(3 * 6 + i) * RCONT_STRIDE] =
+                    DRIFT_PARKED(3, i) =
                         D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
                         D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
                 }
@@ -496,13 +508,13 @@ struct Dop853Lane {
                 double r1[6], r2[6], r3[6], r4[6], r5[6], r6[6], r7[6], r8[6];
 #pragma unroll
                 for (int i = 0; i < 6; i++) {
-                    r5[i] = h * (park[(0 * 6 + i) * RCONT_STRIDE] + D413 * k4[i] + D414 * k10[i] +
+                    r5[i] = h * (DRIFT_PARKED(0, i) + D413 * k4[i] + D414 * k10[i] +
                                  D415 * k2[i] + D416 * k3[i]);
-                    r6[i] = h * (park[(1 * 6 + i) * RCONT_STRIDE] + D513 * k4[i] + D514 * k10[i] +
+                    r6[i] = h * (DRIFT_PARKED(1, i) + D513 * k4[i] + D514 * k10[i] +
                                  D515 * k2[i] + D516 * k3[i]);
-                    r7[i] = h * (park[(2 * 6 + i) * RCONT_STRIDE] + D613 * k4[i] + D614 * k10[i] +
+                    r7[i] = h * (DRIFT_PARKED(2, i) + D613 * k4[i] + D614 * k10[i] +
                                  D615 * k2[i] + D616 * k3[i]);
-                    r8[i] = h * (park[(3 * 6 + i) * RCONT_STRIDE] + D713 * k4[i] + D714 * k10[i] +
+                    r8[i] = h * (DRIFT_PARKED(3, i) + D713 * k4[i] + D714 * k10[i] +
                                  D715 * k2[i] + D716 * k3[i]);
                     r1[i] = y[i];
                     double ydiff = k5[i] - y[i];
@@ -511,6 +523,7 @@ struct Dop853Lane {
                     r3[i] = bspl;
                     r4[i] = ydiff - h * k4[i] - bspl;
                 }
+#undef DRIFT_PARKED
 
                 // Dense output of every requested time strictly before t_current.
 #if !DRIFT_EXACT_ARITH

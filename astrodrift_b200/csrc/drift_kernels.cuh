@@ -99,11 +99,16 @@ __host__ __device__ constexpr bool needs_bulge_table()
 #ifndef DRIFT_MIN_BLOCKS_DOP853
 #define DRIFT_MIN_BLOCKS_DOP853 2
 #endif
+#ifndef DRIFT_MIN_BLOCKS_DOP853_HEAVY
+#define DRIFT_MIN_BLOCKS_DOP853_HEAVY 2
+#endif
 
 template <int METHOD, class Pot>
 struct LaunchShape {
     static constexpr int threads = DRIFT_MAX_THREADS;
-    static constexpr int min_blocks = METHOD == DRIFT_DOP853 ? DRIFT_MIN_BLOCKS_DOP853 : DRIFT_MIN_BLOCKS_PER_SM;
+    static constexpr int min_blocks =
+        METHOD != DRIFT_DOP853 ? DRIFT_MIN_BLOCKS_PER_SM
+                               : (compact_extra_stages<Pot>() ? DRIFT_MIN_BLOCKS_DOP853_HEAVY : DRIFT_MIN_BLOCKS_DOP853);
 };
 
 // Dynamic shared memory per block: the DOP853 rcont parking tile (24
