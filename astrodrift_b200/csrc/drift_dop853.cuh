@@ -12,9 +12,9 @@
 // The state that outlives a step (y, k1 = f(y), h, t, flags) lives in
 // registers; stage vectors are locals of `step` so the compiler can reuse
 // their registers across stages.  On accept the eight-term partial sums of
-// rcont5..8 must survive the three extra stages; they are parked in this
-// thread's column of a shared-memory tile instead of holding 48 registers
-// through the register-heaviest part of the step.
+// rcont5..8 must survive the three extra stages: in registers, or for the
+// heavy forces (whose kernels have fewer registers per thread) parked in
+// this thread's column of a shared-memory tile (RcontPark).
 //
 // DRIFT_EXACT_ARITH (set by the including translation unit): 1 keeps every
 // division of the reference's error norm; 0 multiplies by one reciprocal per
@@ -28,12 +28,6 @@
 
 #ifndef DRIFT_EXACT_ARITH
 #define DRIFT_EXACT_ARITH 1
-#endif
-
-// 1: the eight-term partial sums of rcont5..8 wait out the three extra
-// stages in shared memory (the `park` tile); 0: in registers.
-#ifndef DRIFT_PARK_RCONT
-#define DRIFT_PARK_RCONT 1
 #endif
 
 namespace drift {
@@ -212,6 +206,23 @@ __host__ __device__ constexpr bool compact_extra_stages()
 {
     return std::is_same<Pot, Bovy>::value || std::is_same<Pot, Composite>::value;
 }
+
+// Where the eight-term partial sums of rcont5..8 wait out the three extra
+// stages of an accepted step.  The heavy forces' kernels run three blocks of
+// 128 per SM (168 registers) and park them in this thread's column of a
+// shared-memory tile; the others run two blocks (up to 255 registers), which
+// hold them in registers (the Plummer workload: 67.2 against 70.2 ms per pass).
+struct RcontPark {
+    volatile double *p;
+    int stride;
+    __device__ __forceinline__ void put(int j, int i, double v) { p[(j * 6 + i) * stride] = v; }
+    __device__ __forceinline__ double get(int j, int i) const { return p[(j * 6 + i) * stride]; }
+};
+struct RcontRegs {
+    double v[24];
+    __device__ __forceinline__ void put(int j, int i, double x) { v[j * 6 + i] = x; }
+    __device__ __forceinline__ double get(int j, int i) const { return v[j * 6 + i]; }
+};
 
 template <class Pot>
 struct Dop853Lane {
@@ -419,27 +430,23 @@ struct Dop853Lane {
             const bool skip_dense =
                 sparse_output && !(next < grid.nt - 1 && pos_neg * grid.at(next + 1) < pos_neg * t_new);
             if (!skip_dense) {
-#if DRIFT_PARK_RCONT
-#define DRIFT_PARKED(j, i) park[((j) * 6 + (i)) * RCONT_STRIDE]
-#else
-                double parked[24];
-#define DRIFT_PARKED(j, i) parked[(j) * 6 + (i)]
-#endif
+                std::conditional_t<compact_extra_stages<Pot>(), RcontPark, RcontRegs> parked;
+                if constexpr (compact_extra_stages<Pot>()) parked = RcontPark{park, RCONT_STRIDE};
 
 #pragma unroll
                 for (int i = 0; i < 6; i++) {
-                    DRIFT_PARKED(0, i) =
+                    parked.put(0, i,
                         D41 * k1[i] + D46 * k6[i] + D47 * k7[i] + D48 * k8[i] + D49 * k9[i] +
-                        D410 * k10[i] + D411 * k2[i] + D412 * k3[i];
-                    DRIFT_PARKED(1, i) =
+                        D410 * k10[i] + D411 * k2[i] + D412 * k3[i]);
+                    parked.put(1, i,
                         D51 * k1[i] + D56 * k6[i] + D57 * k7[i] + D58 * k8[i] + D59 * k9[i] +
-                        D510 * k10[i] + D511 * k2[i] + D512 * k3[i];
-                    DRIFT_PARKED(2, i) =
+                        D510 * k10[i] + D511 * k2[i] + D512 * k3[i]);
+                    parked.put(2, i,
                         D61 * k1[i] + D66 * k6[i] + D67 * k7[i] + D68 * k8[i] + D69 * k9[i] +
-                        D610 * k10[i] + D611 * k2[i] + D612 * k3[i];
-                    DRIFT_PARKED(3, i) =
+                        D610 * k10[i] + D611 * k2[i] + D612 * k3[i]);
+                    parked.put(3, i,
                         D71 * k1[i] + D76 * k6[i] + D77 * k7[i] + D78 * k8[i] + D79 * k9[i] +
-                        D710 * k10[i] + D711 * k2[i] + D712 * k3[i];
+                        D710 * k10[i] + D711 * k2[i] + D712 * k3[i]);
                 }
                 if constexpr (compact_extra_stages<Pot>()) {
                     // Stages 14..16 around one force call site: for the heavy
@@ -508,13 +515,13 @@ struct Dop853Lane {
                 double r1[6], r2[6], r3[6], r4[6], r5[6], r6[6], r7[6], r8[6];
 #pragma unroll
                 for (int i = 0; i < 6; i++) {
-                    r5[i] = h * (DRIFT_PARKED(0, i) + D413 * k4[i] + D414 * k10[i] +
+                    r5[i] = h * (parked.get(0, i) + D413 * k4[i] + D414 * k10[i] +
                                  D415 * k2[i] + D416 * k3[i]);
-                    r6[i] = h * (DRIFT_PARKED(1, i) + D513 * k4[i] + D514 * k10[i] +
+                    r6[i] = h * (parked.get(1, i) + D513 * k4[i] + D514 * k10[i] +
                                  D515 * k2[i] + D516 * k3[i]);
-                    r7[i] = h * (DRIFT_PARKED(2, i) + D613 * k4[i] + D614 * k10[i] +
+                    r7[i] = h * (parked.get(2, i) + D613 * k4[i] + D614 * k10[i] +
                                  D615 * k2[i] + D616 * k3[i]);
-                    r8[i] = h * (DRIFT_PARKED(3, i) + D713 * k4[i] + D714 * k10[i] +
+                    r8[i] = h * (parked.get(3, i) + D713 * k4[i] + D714 * k10[i] +
                                  D715 * k2[i] + D716 * k3[i]);
                     r1[i] = y[i];
                     double ydiff = k5[i] - y[i];
@@ -523,7 +530,6 @@ struct Dop853Lane {
                     r3[i] = bspl;
                     r4[i] = ydiff - h * k4[i] - bspl;
                 }
-#undef DRIFT_PARKED
 
                 // Dense output of every requested time strictly before t_current.
 #if !DRIFT_EXACT_ARITH

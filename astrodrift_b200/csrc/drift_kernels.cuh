@@ -82,12 +82,16 @@ __host__ __device__ constexpr bool needs_bulge_table()
 // threads per block, and registers allocated so that a given number of such
 // blocks can be resident on one SM.  Registers are allocated per scheduler
 // (16K each), so the choices are two warps per scheduler (up to 255
-// registers), three (168) or four (128).
-//   DOP853: DRIFT_MIN_BLOCKS_DOP853 = 2 blocks of 128.  Its step needs about
-//     250 registers; with them and no spills two warps per scheduler beat
-//     three warps that spill: the uneven Bovy workload's 2^18-particle slice
-//     0.87 s against 1.18 s per pass (4 blocks: 1.55 s), the Plummer workload
-//     70.8 against 71.7 ms.
+// registers), three (168) or four (128).  Measured on full workloads
+// (throughput, not the tail of a slice):
+//   DOP853, light forces: DRIFT_MIN_BLOCKS_DOP853 = 2 blocks of 128; the step
+//     fits in about 250 registers with rcont5..8 held in registers (the
+//     Plummer workload, 2^20 particles: 67.2 ms per pass, against 70.2 ms
+//     with them parked in shared memory and 71.7 ms at 3 blocks).
+//   DOP853, Bovy and force models: DRIFT_MIN_BLOCKS_DOP853_HEAVY = 3 (168
+//     registers, a few hundred bytes of spills): the uneven Bovy workload,
+//     2^22 particles, 12.36 s per pass against 12.93 s at 2 blocks (a
+//     2^18-particle slice, whose pass is its slowest particle, prefers 2).
 //   DOPR54: DRIFT_MIN_BLOCKS_PER_SM = 3 (the Kepler configuration: 7.15 ms
 //     against 7.22 ms at 2).
 #ifndef DRIFT_MAX_THREADS
@@ -100,7 +104,7 @@ __host__ __device__ constexpr bool needs_bulge_table()
 #define DRIFT_MIN_BLOCKS_DOP853 2
 #endif
 #ifndef DRIFT_MIN_BLOCKS_DOP853_HEAVY
-#define DRIFT_MIN_BLOCKS_DOP853_HEAVY 2
+#define DRIFT_MIN_BLOCKS_DOP853_HEAVY 3
 #endif
 
 template <int METHOD, class Pot>
