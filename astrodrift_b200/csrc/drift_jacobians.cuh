@@ -9,7 +9,8 @@
 //   Plummer:             amp, b
 //   Bovy:                mn_amp, mn_a, mn_b, nfw_amp, nfw_a, bulge_k
 // Used by the adjoint only, which is compiled with contraction: powers,
-// logs, exps and reciprocals are the few-ulp forms of drift_math.cuh.
+// logs, exps, inverse square roots and reciprocals are the few-ulp forms of
+// drift_math.cuh (ln and exp from the tables staged beside the bulge table).
 // The formulas are the analytic derivatives of the forces in
 // drift_potentials.cuh (shared/src/potential.rs:126-176, 229-262 and the
 // galpy-cylindrical Kepler force of src/integrators/galpy/dopr54.rs:75-88,
@@ -92,13 +93,14 @@ struct BovyJac {
     __device__ __forceinline__ void vjp(double x, double y, double z, const double *w, double *jw,
                                         double *dp) const
     {
+        const double *T = table + BULGE_TABLE_SIZE;  // ln / exp tables (drift_math.cuh)
         const double xw = x * w[0] + y * w[1] + z * w[2];
         const double r2 = x * x + y * y + z * z;
         jw[0] = jw[1] = jw[2] = 0.0;
         // disk
         {
             double zeta2 = z * z + mn_b * mn_b;
-            double izeta = rsqrt(zeta2);
+            double izeta = rsqrt_few_ulp(zeta2);
             double zeta = zeta2 * izeta;
             double A = mn_a + zeta;
             double D = x * x + y * y + A * A;
@@ -117,7 +119,7 @@ struct BovyJac {
                                 3.0 * A * mn_b * izeta * d25 * gw);
         }
         if (r2 != 0.0) {
-            const double inv_r = rsqrt(r2);
+            const double inv_r = rsqrt_few_ulp(r2);
             const double r = r2 * inv_r;
             const double ir3 = inv_r * inv_r * inv_r;
             const double c3 = 3.0 * xw * ir3 * (inv_r * inv_r);
@@ -125,7 +127,7 @@ struct BovyJac {
             {
                 double apr = nfw_a + r;
                 double inv_apr = fast_rcp(apr);
-                double m = unit_log(1.0 + r * inv_nfw_a) - r * inv_apr;
+                double m = log_tab(T, 1.0 + r * inv_nfw_a) - r * inv_apr;
                 double e = xw * ir3 * (inv_apr * inv_apr);
                 jw[0] += -nfw_amp * (m * (w[0] * ir3 - x * c3) + x * e);
                 jw[1] += -nfw_amp * (m * (w[1] * ir3 - y * c3) + y * e);
@@ -137,7 +139,7 @@ struct BovyJac {
             {
                 double u = r2 * inv_rc2;
                 double G = bulge_lower_gamma(table, bulge_s, u, bulge_gamma_s);
-                double Gp = unit_exp((bulge_s - 1.0) * unit_log(u) - u) * 2.0 * r * inv_rc2;
+                double Gp = exp_tab(T, (bulge_s - 1.0) * log_tab(T, u) - u) * 2.0 * r * inv_rc2;
                 double e = Gp * xw * ir3 * inv_r;
                 jw[0] += -bulge_k * (G * (w[0] * ir3 - x * c3) + x * e);
                 jw[1] += -bulge_k * (G * (w[1] * ir3 - y * c3) + y * e);

@@ -39,7 +39,10 @@ struct Segment {
 // skips the dense-output stages of steps that emit no sample.  (With dense
 // grids most warps emit somewhere in most steps, and warps that take and
 // skip the block at different times thrash the instruction cache.)
-constexpr int SPARSE_OUTPUT_NT = 8;
+#ifndef DRIFT_SPARSE_OUTPUT_NT
+#define DRIFT_SPARSE_OUTPUT_NT 8
+#endif
+constexpr int SPARSE_OUTPUT_NT = DRIFT_SPARSE_OUTPUT_NT;
 
 // Everything a launch needs, passed by value as the kernel parameter.
 struct KernelArgs {
