@@ -114,6 +114,7 @@ struct DeviceContext {
     int sm_count = 0;
     std::mutex mu;  // serialises host-buffer calls that share the buffers below
     cudaStream_t streams[2] = {nullptr, nullptr};
+    cudaStream_t poll_stream = nullptr;  // streamed copy-out: reads the chunk counters
     cudaEvent_t done[2] = {nullptr, nullptr};
     DevBuf y0, grid, out[2], yfin, status, err, acc, rej, cursor, origins;
     DevBuf src_traj, src_table, src_origins;  // drift_origin_table_host
@@ -139,6 +140,11 @@ struct DeviceContext {
             if (streams[i]) cudaStreamSynchronize(streams[i]);
         for (DevBuf *d : dev_bufs) d->release();
         poll.release();
+        if (poll_stream) {
+            cudaStreamSynchronize(poll_stream);
+            cudaStreamDestroy(poll_stream);
+            poll_stream = nullptr;
+        }
         for (int i = 0; i < 2; i++) {
             stage[i].release();
             if (done[i]) cudaEventDestroy(done[i]);
@@ -182,6 +188,7 @@ int DeviceContext::init(int dev)
         DRIFT_CUDA_TRY(cudaStreamCreateWithFlags(&streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
         DRIFT_CUDA_TRY(cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming), "cudaEventCreate");
     }
+    DRIFT_CUDA_TRY(cudaStreamCreateWithFlags(&poll_stream, cudaStreamNonBlocking), "cudaStreamCreate");
     return DRIFT_SUCCESS;
 }
 
@@ -833,9 +840,26 @@ int drift_host_free(void *ptr)
 static int host_integrate(DeviceContext *ctx, const drift_launch *L);
 
 // Requests above this many particles may take the streamed copy-out.
-constexpr int64_t STREAMED_MIN_PARTICLES = 65536;
-// Particle chunks of a streamed copy-out.
+#ifndef DRIFT_STREAMED_MIN_PARTICLES
+#define DRIFT_STREAMED_MIN_PARTICLES 65536
+#endif
+constexpr int64_t STREAMED_MIN_PARTICLES = DRIFT_STREAMED_MIN_PARTICLES;
+// Particle chunks of a streamed copy-out: between STREAMED_MIN_CHUNKS and
+// STREAMED_CHUNKS, each holding about STREAMED_PER_LANE particles per
+// resident thread, so that a chunk lasts many particle lifetimes and the
+// particles that must go first (those that outlast a chunk's share of the
+// launch) stay few.  Measured end to end with page-locked buffers: the
+// uneven Bovy workload (2^22 particles, compute-bound) 13.04 s per pass at
+// 4 particles per thread per chunk (18 chunks), 12.54 s at 16 (4 chunks),
+// against 12.29 s for the device pass alone; the Plummer workload (2^20
+// particles, bound by the 10 GB device-to-host copy) 217 ms at 6 chunks and
+// 275 ms at 1 chunk, whose copy then waits for the whole launch.
 constexpr int STREAMED_CHUNKS = 32;
+constexpr int STREAMED_MIN_CHUNKS = 4;
+#ifndef DRIFT_STREAMED_PER_LANE
+#define DRIFT_STREAMED_PER_LANE 16
+#endif
+constexpr int64_t STREAMED_PER_LANE = DRIFT_STREAMED_PER_LANE;
 
 static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 
@@ -845,13 +869,15 @@ static size_t align256(size_t b) { return (b + 255) / 256 * 256; }
 // (drift::build_order_chunked) runs the particles that outlast a chunk's
 // share of the launch first, then chunk 0's particles longest first, then
 // chunk 1's, and so on, and every particle counts itself done in its chunk's
-// counter.  This thread reads the counters back every 200 microseconds (a
-// small copy on the second stream) and copies each finished chunk's
-// trajectory to the caller as soon as its counter is full, so the copy-out
-// overlaps the rest of the launch and only the last chunks' copies remain
-// after it.  The loop ends when every chunk is copied; once the launch's
-// completion event fires, whatever is left is copied at once, so a launch
-// that ends early (an error, a timeout) never leaves the loop waiting.
+// counter (4 to 32 chunks, see STREAMED_PER_LANE).  This thread reads the
+// counters back every 200 microseconds (a small copy on a stream of its own,
+// so that reading never waits behind a chunk's copy) and queues each
+// finished chunk's trajectory copy on the second stream as soon as its
+// counter is full, so the copy-out overlaps the rest of the launch and only
+// the last chunks' copies remain after it.  The loop ends when every chunk
+// is copied; once the launch's completion event fires, whatever is left is
+// copied at once, so a launch that ends early (an error, a timeout) never
+// leaves the loop waiting.
 static int stream_copy_out(DeviceContext *ctx, const drift_launch *L)
 {
     drift::TraceRange trace("drift host streamed copy-out");
@@ -860,7 +886,16 @@ static int stream_copy_out(DeviceContext *ctx, const drift_launch *L)
     const size_t row = 6 * sizeof(double);
     cudaStream_t s0 = ctx->streams[0], s1 = ctx->streams[1];
 
-    const int64_t chunk_len = ((n + STREAMED_CHUNKS - 1) / STREAMED_CHUNKS + 127) / 128 * 128;
+    drift_launch shape = *L;
+    shape.schedule = DRIFT_SCHEDULE_ORDERED;
+    const int block = block_of(&shape);
+    int grid = 0;
+    int rc = grid_for(ctx->sm_count, &shape, n, block, &grid);
+    if (rc) return rc;
+    const int64_t lanes = (int64_t)grid * block;
+    const int64_t want = std::max<int64_t>(STREAMED_MIN_CHUNKS,
+                                           std::min<int64_t>(STREAMED_CHUNKS, n / (lanes * STREAMED_PER_LANE)));
+    const int64_t chunk_len = ((n + want - 1) / want + 127) / 128 * 128;
     const int nchunks = (int)((n + chunk_len - 1) / chunk_len);
     const size_t scratch = drift::chunked_order_scratch(nchunks);
     const size_t ws = CURSOR_BYTES + scratch + align256(nchunks * sizeof(unsigned)) + align256(4 * (size_t)n) +
@@ -917,21 +952,17 @@ static int stream_copy_out(DeviceContext *ctx, const drift_launch *L)
     uint32_t *order = reinterpret_cast<uint32_t *>(reinterpret_cast<char *>(done) + align256(nchunks * sizeof(unsigned)));
     uint8_t *keys = reinterpret_cast<uint8_t *>(order) + align256(4 * (size_t)n);
     drift::KernelArgs a = make_args(&sub);
-    const int block = block_of(&sub);
-    int grid = 0;
-    int rc = grid_for(ctx->sm_count, &sub, n, block, &grid);
-    if (rc) return rc;
     a.persistent = 1;
     a.cursor = reinterpret_cast<unsigned long long *>(base);
     a.chunk_done = done;
     a.chunk_len = chunk_len;
     DRIFT_CUDA_TRY(cudaMemsetAsync(base, 0, sizeof(unsigned long long), s0), "cudaMemsetAsync");
     DRIFT_CUDA_TRY(cudaMemsetAsync(done, 0, nchunks * sizeof(unsigned), s0), "cudaMemsetAsync");
-    // stream 1 reads the counters only after they are cleared
+    // the counters are read (poll stream) only after they are cleared
     DRIFT_CUDA_TRY(cudaEventRecord(ctx->done[1], s0), "cudaEventRecord");
-    DRIFT_CUDA_TRY(cudaStreamWaitEvent(s1, ctx->done[1], 0), "cudaStreamWaitEvent");
+    DRIFT_CUDA_TRY(cudaStreamWaitEvent(ctx->poll_stream, ctx->done[1], 0), "cudaStreamWaitEvent");
     DRIFT_CUDA_TRY(drift::build_order_chunked(a, sub.method, keys, counts, split, chunk_counts, order, chunk_len,
-                                              nchunks, (int64_t)grid * block, ctx->sm_count, s0),
+                                              nchunks, lanes, ctx->sm_count, s0),
                    "ordering kernels");
     a.order = order;
     DRIFT_CUDA_TRY(launch_args(a, sub.method, sub.precision, grid, block, s0), "kernel launch");
@@ -949,9 +980,10 @@ static int stream_copy_out(DeviceContext *ctx, const drift_launch *L)
             DRIFT_CUDA_TRY(cudaStreamWaitEvent(s1, ctx->done[0], 0), "cudaStreamWaitEvent");
         } else {
             cudaGetLastError();  // clears the not-ready status
-            DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->poll.ptr, done, nchunks * sizeof(unsigned), cudaMemcpyDeviceToHost, s1),
+            DRIFT_CUDA_TRY(cudaMemcpyAsync(ctx->poll.ptr, done, nchunks * sizeof(unsigned), cudaMemcpyDeviceToHost,
+                                           ctx->poll_stream),
                            "D2H chunk counters");
-            DRIFT_CUDA_TRY(cudaStreamSynchronize(s1), "cudaStreamSynchronize");
+            DRIFT_CUDA_TRY(cudaStreamSynchronize(ctx->poll_stream), "cudaStreamSynchronize");
         }
         for (int c = 0; c < nchunks; c++) {
             if (copied[c]) continue;

@@ -567,8 +567,9 @@ def e2e_leg(args, capi, torch, method, pot, y0, ts, t_end, nt, tol, precision, s
         elapsed = reduce_max(elapsed, dist, dev)
     ok = bool(np.array_equal(out_p[nt - 1], out_last_device))
     # the copy roofline of this leg: pinned device->host bandwidth (1 GiB copies)
-    probe = torch.empty(1 << 27, dtype=torch.float64, device=dev)
-    host_probe = torch.from_numpy(out_p.reshape(-1)[: (1 << 27)])
+    probe_n = min(1 << 27, out_p.size)
+    probe = torch.empty(probe_n, dtype=torch.float64, device=dev)
+    host_probe = torch.from_numpy(out_p.reshape(-1)[:probe_n])
     d2h = []
     for _ in range(3):
         a_, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -588,7 +589,8 @@ def e2e_leg(args, capi, torch, method, pot, y0, ts, t_end, nt, tol, precision, s
            "copy_roofline": {"bound": "pcie_d2h", "peak_gbs": d2h_gbs,
                              "achieved_gbs": out_bytes * args.e2e_steps / elapsed / 1e9,
                              "frac": out_bytes * args.e2e_steps / elapsed / 1e9 / d2h_gbs,
-                             "peak_source": "pinned 1 GiB device->host copies measured in this run"}}
+                             "peak_source": f"pinned {probe_n * 8 / 2**30:.3g} GiB device->host copies measured "
+                                            "in this run"}}
     del y0_p, grid_p, out_p, per
     for ptr in bufs.values():
         lib.drift_host_free(ptr)
