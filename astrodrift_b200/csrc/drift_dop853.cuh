@@ -233,6 +233,7 @@ struct Dop853Lane {
     double hmax;
     double pos_neg;
     int32_t next;         // finished_user_t_ii
+    double t_next;        // output time next + 1 (valid while next < nt - 1)
     int32_t reject;
     int32_t nonfinite_run;
     bool done;
@@ -289,6 +290,7 @@ struct Dop853Lane {
         h = custom_sign(c_min(100.0 * fabs(hh), c_min(fabs(h1), fabs(hmax))), pos_neg);
         reject = 0;
         next = 0;
+        t_next = grid.nt > 1 ? grid.at(1) : 0.0;
         nonfinite_run = 0;
         t_cur = t0;
     }
@@ -428,7 +430,7 @@ struct Dop853Lane {
             // with no requested time in (t_old, t_new) skips them; emitted
             // samples are unchanged.
             const bool skip_dense =
-                sparse_output && !(next < grid.nt - 1 && pos_neg * grid.at(next + 1) < pos_neg * t_new);
+                sparse_output && !(next < grid.nt - 1 && pos_neg * t_next < pos_neg * t_new);
             if (!skip_dense) {
                 std::conditional_t<compact_extra_stages<Pot>(), RcontPark, RcontRegs> parked;
                 if constexpr (compact_extra_stages<Pot>()) parked = RcontPark{park, RCONT_STRIDE};
@@ -535,8 +537,11 @@ struct Dop853Lane {
 #if !DRIFT_EXACT_ARITH
                 const double inv_h = fast_rcp(h);
 #endif
+                // The next output time is formed once per emitted sample
+                // (t_next), not once per step: for per-particle grids that
+                // is a division (OutputGrid::sample) saved in every step.
                 while (next < grid.nt - 1) {
-                    double tk = grid.at(next + 1);
+                    const double tk = t_next;
                     if (!(pos_neg * tk < pos_neg * t_new)) break;
 #if DRIFT_EXACT_ARITH
                     double s = (tk - t_old) / h;
@@ -554,6 +559,7 @@ struct Dop853Lane {
                                                 s1 * (r5[i] + s * (r6[i] + s1 * (r7[i] + s * r8[i]))))));
                     out.write(next + 1, yy);
                     next += 1;
+                    if (next < grid.nt - 1) t_next = grid.at(next + 1);
                 }
             }
 #pragma unroll
