@@ -12,8 +12,9 @@
 //                   exponential cutoff (enclosed-mass force).  In FMA mode
 //                   (DRIFT_EXACT_ARITH 0) the disk and halo use reciprocals
 //                   and a few-ulp rsqrt instead of the reference's
-//                   divisions, the bulge and halo share one inverse radius,
-//                   and ln / exp come from shared-memory tables.
+//                   divisions, the bulge and halo share one inverse radius
+//                   and one radial sum, and ln / exp come from shared-memory
+//                   tables.
 // pow(., -1.5) and pow(., 1.5) go through the routines of drift_math.cuh
 // instead of a general pow: correctly rounded in the exact unit, within a
 // few ulps in the contraction unit, which also takes the Bovy force's log
@@ -246,48 +247,42 @@ struct Bovy {
             hy = ar * (y / r);
             hz = ar * (z / r);
         }
-#else
-        // One inverse radius serves the bulge and the halo.
-        const double r2s = x * x + y * y + z * z;
-        const double inv_r = rsqrt_few_ulp(r2s);
-        const double inv_r3 = inv_r * inv_r * inv_r;
-        // bulge
-        double bx = 0.0, by = 0.0, bz = 0.0;
-        if (r2s != 0.0) {
-            const double g = bulge_lower_gamma(table, bulge_s, r2s * inv_rc2, bulge_gamma_s);
-            const double ar_over_r = -bulge_k * g * inv_r3;
-            bx = ar_over_r * x;
-            by = ar_over_r * y;
-            bz = ar_over_r * z;
-        }
-        // Miyamoto-Nagai disk: a_R x/R == -amp x / D with
-        // D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
-        double dx, dy, dz;
-        {
-            const double r2 = x * x + y * y;
-            const double zb2 = z * z + mn_b2;
-            const double inv_sz = rsqrt_few_ulp(zb2);
-            const double apz = fma(zb2, inv_sz, mn_a);
-            const double m_over_d = -mn_amp * unit_pow_m1p5(fma(apz, apz, r2));
-            dx = m_over_d * x;
-            dy = m_over_d * y;
-            dz = m_over_d * z * apz * inv_sz;
-        }
-        // NFW halo
-        double hx, hy, hz;
-        {
-            const double r = r2s * inv_r;
-            const double u = r * inv_nfw_a;
-            const double term = log_tab(table + BULGE_TABLE_SIZE, 1. + u) - u * fast_rcp(1.0 + u);
-            const double ar_over_r = -nfw_amp * term * inv_r3;
-            hx = ar_over_r * x;
-            hy = ar_over_r * y;
-            hz = ar_over_r * z;
-        }
-#endif
         ax = (bx + dx) + hx;
         ay = (by + dy) + hy;
         az = (bz + dz) + hz;
+#else
+        // One inverse radius serves the bulge and the halo, whose radial
+        // accelerations are summed into one a_r / r before the disk is added
+        // (fewer live temporaries than three separate vectors: the uneven
+        // Bovy workload 12.40 -> 12.15 s per pass).
+        const double r2s = x * x + y * y + z * z;
+        const double inv_r = rsqrt_few_ulp(r2s);
+        const double inv_r3 = inv_r * inv_r * inv_r;
+        double ar_over_r;
+        {
+            // NFW halo
+            const double r = r2s * inv_r;
+            const double u = r * inv_nfw_a;
+            const double term = log_tab(table + BULGE_TABLE_SIZE, 1. + u) - u * fast_rcp(1.0 + u);
+            ar_over_r = -nfw_amp * term;
+        }
+        if (r2s != 0.0) {
+            // bulge
+            const double g = bulge_lower_gamma(table, bulge_s, r2s * inv_rc2, bulge_gamma_s);
+            ar_over_r = fma(-bulge_k, g, ar_over_r);
+        }
+        ar_over_r *= inv_r3;
+        // Miyamoto-Nagai disk: a_R x/R == -amp x / D with
+        // D = (R^2 + (a + sqrt(z^2 + b^2))^2)^(3/2)
+        const double r2 = x * x + y * y;
+        const double zb2 = z * z + mn_b2;
+        const double inv_sz = rsqrt_few_ulp(zb2);
+        const double apz = fma(zb2, inv_sz, mn_a);
+        const double m_over_d = -mn_amp * unit_pow_m1p5(fma(apz, apz, r2));
+        ax = (m_over_d + ar_over_r) * x;
+        ay = (m_over_d + ar_over_r) * y;
+        az = fma(m_over_d * apz, z * inv_sz, ar_over_r * z);
+#endif
     }
 };
 
