@@ -706,6 +706,7 @@ def serving_short_pass(args) -> dict:
     cap = args.trajectory_cap_mib << 20
     _warm_server_kernels(capi, precision)
     calib = serving_requests(args.serving_requests, args.seed, capi)
+    _serial(capi, calib, cap, precision)  # warm: grows the host path's buffers, as the server's pool is warmed
     t_serial, acc_serial, _ = _serial(capi, calib, cap, precision)
     with Server(memory_fraction=0.6, streams=args.streams) as srv:
         _serve(srv, calib, cap, precision, open_loop=False)  # warms the pool
@@ -730,7 +731,8 @@ def run_serving(args) -> None:
 
     A seeded calibration set of --serving-requests requests is run (i) one
     drift_integrate_host call at a time under the plain schedule (the serial
-    plain-launch baseline) and (ii) all submitted at once to the server
+    plain-launch baseline; one untimed pass first grows the host path's
+    buffers) and (ii) all submitted at once to the server
     (saturated, continuous batching; median of three passes after a warm-up
     pass), which gives the capacity in requests/s.  Then, for each offered
     load in --loads, a fresh seeded Poisson stream at that fraction of the
@@ -754,6 +756,7 @@ def run_serving(args) -> None:
     _warm_server_kernels(capi, precision)
     calib = serving_requests(args.serving_requests, args.seed, capi)
     log(f"serving: {len(calib)} calibration requests, {sum(len(r['y0']) for r in calib)} particles")
+    _serial(capi, calib, cap, precision)  # warm: grows the host path's buffers, as the server's pool is warmed
     t_serial, acc_serial, alone = _serial(capi, calib, cap, precision)
     log(f"serving: serial {t_serial:.2f} s")
     gpu = gpu_uuid(torch, torch.device(f"cuda:{local}"))
