@@ -110,10 +110,12 @@ def test_kepler_corpus_matches_oracle(oracle, cuda_device, method, precision):
     # OutputGrid sampling only in the last bit of some output times)
     assert rel_err(got["out"][-1], g[f"{method}_final"]) < REL_TOL
     same = (got["accepted"].astype(np.int64) == ref["accepted"]).mean()
+    print(f"Kepler corpus {method} precision {precision}: identical accepted-step counts {same:.4f}")
+    # measured: every particle's count identical in both units
     if precision == capi.EXACT:
-        assert same >= 0.98, same
+        assert same == 1.0, same
     else:
-        assert same >= 0.9, same
+        assert same >= 0.99, same
 
 
 # ---------------------------------------------------------------- potentials
@@ -141,7 +143,10 @@ def test_potential_batches_match_oracle(oracle, cuda_device, pname, method, prec
     assert rel_err(got["out"], ref["out"]) < tol
     np.testing.assert_array_equal(got["y_final"], got["out"][-1])
     same = (got["accepted"].astype(np.int64) == g[f"{pname}_{method}_accepted"]).mean()
-    assert same >= (0.95 if precision == capi.EXACT else 0.85), same
+    print(f"{pname} {method} precision {precision} schedule {schedule}: identical accepted-step counts {same:.4f}")
+    # measured: all identical in the exact unit; the contraction unit 98.4 % for Bovy DOP853
+    # (one particle in 64), all identical otherwise
+    assert same >= (1.0 if precision == capi.EXACT else 0.97), same
 
 
 @pytest.mark.parametrize("method", ["dopr54", "dop853"])
