@@ -634,13 +634,46 @@ def serving_requests(count, seed, capi, arrival_rate=None):
     return reqs
 
 
-def _serve(srv, reqs, cap_bytes, precision, open_loop: bool):
+class ResultSlots:
+    """Page-locked result buffers of cap_bytes each (drift_host_alloc), reused
+    across requests, as a serving client keeps them: results then copy at the
+    device-to-host rate instead of through the driver's pageable staging and
+    first-touch page faults."""
+
+    def __init__(self, count: int, cap_bytes: int):
+        from astrodrift_b200.serving import PinnedArray
+
+        self.bufs = [PinnedArray((cap_bytes // 8,)) for _ in range(count)]
+        self.free = list(range(count))
+
+    def view(self, slot: int, nt: int, n: int) -> np.ndarray:
+        return self.bufs[slot].array[: nt * n * 6].reshape(nt, n, 6)
+
+    def close(self) -> None:
+        for b in self.bufs:
+            b.free()
+
+
+def _serve(srv, reqs, cap_bytes, precision, open_loop: bool, slots: ResultSlots):
     """Submit every request (at its arrival time when open_loop, else all at
-    once); returns (seconds, accepted steps, latencies s, capped count).
-    Results come back into pageable numpy buffers; a request whose trajectory
-    exceeds cap_bytes returns its final states only (its integration, dense
-    output included, is unchanged; the samples are not stored)."""
-    handles, capped = [], 0
+    once); returns (seconds, accepted steps, latencies s, capped count, client
+    waits s).  Results come back into the page-locked slots; when all are in
+    use the client first waits for its oldest request (the wait is recorded;
+    the request's own latency runs from its submission).  A request whose
+    trajectory exceeds cap_bytes returns its final states only (its
+    integration, dense output included, is unchanged; the samples are not
+    stored)."""
+    inflight, lat, waits, capped, acc = [], [], [], 0, 0
+
+    def retire():
+        nonlocal acc
+        h, slot = inflight.pop(0)
+        res = h.wait(timeout=3600.0)
+        lat.append(res["latency_s"])
+        acc += int(res["accepted"].astype(np.int64).sum())
+        if slot is not None:
+            slots.free.append(slot)
+
     t_begin = time.perf_counter()
     for r in reqs:
         if open_loop:
@@ -650,21 +683,26 @@ def _serve(srv, reqs, cap_bytes, precision, open_loop: bool):
         n, nt = len(r["y0"]), r["nt"]
         want = nt * n * 48 <= cap_bytes
         capped += not want
+        slot = None
+        if want:
+            t_want = time.perf_counter()
+            while not slots.free:
+                retire()
+            waits.append(time.perf_counter() - t_want)
+            slot = slots.free.pop()
         h = srv.submit(r["method"], r["pot"], r["y0"], ts=np.linspace(0.0, r["t_end"], nt), rtol=r["rtol"],
                        atol=r["rtol"], precision=precision, want_out=want,
-                       out=np.empty((nt, n, 6)) if want else None)
-        handles.append(h)
-    lat, acc = [], 0
-    for h in handles:
-        res = h.wait(timeout=3600.0)
-        lat.append(res["latency_s"])
-        acc += int(res["accepted"].astype(np.int64).sum())
-    return time.perf_counter() - t_begin, acc, lat, capped
+                       out=slots.view(slot, nt, n) if want else None)
+        inflight.append((h, slot))
+    while inflight:
+        retire()
+    return time.perf_counter() - t_begin, acc, lat, capped, waits
 
 
-def _serial(capi, reqs, cap_bytes, precision):
+def _serial(capi, reqs, cap_bytes, precision, slots: ResultSlots):
     """One drift_integrate_host call per request, plain schedule, one after
-    another: the serial plain-launch baseline (and each request's time alone)."""
+    another, results into a page-locked slot: the serial plain-launch
+    baseline (and each request's time alone)."""
     alone, acc = [], 0
     t0 = time.perf_counter()
     for r in reqs:
@@ -673,7 +711,7 @@ def _serial(capi, reqs, cap_bytes, precision):
         ti = time.perf_counter()
         res = capi.integrate_host(r["method"], r["pot"], r["y0"], ts=np.linspace(0.0, r["t_end"], nt),
                                   rtol=r["rtol"], atol=r["rtol"], precision=precision, schedule=capi.PLAIN,
-                                  want_out=want)
+                                  want_out=want, out=slots.view(0, nt, n) if want else None)
         alone.append(time.perf_counter() - ti)
         acc += int(res["accepted"].astype(np.int64).sum())
     return time.perf_counter() - t0, acc, alone
@@ -706,19 +744,25 @@ def serving_short_pass(args) -> dict:
     cap = args.trajectory_cap_mib << 20
     _warm_server_kernels(capi, precision)
     calib = serving_requests(args.serving_requests, args.seed, capi)
-    _serial(capi, calib, cap, precision)  # warm: grows the host path's buffers, as the server's pool is warmed
-    t_serial, acc_serial, _ = _serial(capi, calib, cap, precision)
-    with Server(memory_fraction=0.6, streams=args.streams) as srv:
-        _serve(srv, calib, cap, precision, open_loop=False)  # warms the pool
-        t_sat, acc_sat, _, _ = _serve(srv, calib, cap, precision, open_loop=False)
-        rate = 0.5 * len(calib) / t_sat
-        stream = serving_requests(max(8, int(rate * args.serving_seconds)), args.seed + 1, capi, arrival_rate=rate)
-        t_run, acc_run, lat, capped = _serve(srv, stream, cap, precision, open_loop=True)
+    slots = ResultSlots(args.result_buffers, cap)
+    try:
+        _serial(capi, calib, cap, precision, slots)  # warm, as the server's pool is warmed
+        t_serial, acc_serial, _ = _serial(capi, calib, cap, precision, slots)
+        with Server(memory_fraction=0.6, streams=args.streams) as srv:
+            _serve(srv, calib, cap, precision, False, slots)  # warms the pool
+            t_sat, acc_sat, _, _, _ = _serve(srv, calib, cap, precision, False, slots)
+            rate = 0.5 * len(calib) / t_sat
+            stream = serving_requests(max(8, int(rate * args.serving_seconds)), args.seed + 1, capi,
+                                      arrival_rate=rate)
+            t_run, acc_run, lat, capped, waits = _serve(srv, stream, cap, precision, True, slots)
+    finally:
+        slots.close()
     pct = _pct(lat)
     res = {"p50_ms": pct["p50"], "p99_ms": pct["p99"], "vs_serial": (acc_sat / t_sat) / (acc_serial / t_serial),
            "saturated_value": acc_sat / t_sat, "serial_value": acc_serial / t_serial,
            "open_loop": {"rate_per_s": rate, "offered_load": 0.5, "requests": len(stream), "seconds": t_run,
-                         "accepted_steps_per_s": acc_run / t_run, "latency_ms": pct, "capped_requests": capped},
+                         "accepted_steps_per_s": acc_run / t_run, "latency_ms": pct, "capped_requests": capped,
+                         "client_buffer_wait_ms_p99": float(np.percentile(np.array(waits) * 1e3, 99)) if waits else 0.0},
            "calibration_requests": len(calib),
            "note": "short pass; --workload serving sweeps three rates for 60 s each"}
     log(f"serving: p50 {pct['p50']:.1f} ms p99 {pct['p99']:.1f} ms, {res['vs_serial']:.2f}x serial")
@@ -737,10 +781,13 @@ def run_serving(args) -> None:
     pass), which gives the capacity in requests/s.  Then, for each offered
     load in --loads, a fresh seeded Poisson stream at that fraction of the
     capacity arrives for --stream-seconds seconds; every request's latency
-    (submission to results in host memory) is recorded.  Requests whose
-    trajectory exceeds --trajectory-cap-mib return final states only: their
-    integration (dense output included) is unchanged, the samples are not
-    stored, and the line reports how many requests that touched.
+    (submission to results in host memory) is recorded.  Results go to
+    --result-buffers page-locked buffers reused across requests, as a serving
+    client keeps them (a client whose buffers are all in use waits for its
+    oldest request; the line reports that wait).  Requests whose trajectory
+    exceeds --trajectory-cap-mib return final states only: their integration
+    (dense output included) is unchanged, the samples are not stored, and the
+    line reports how many requests that touched.
     """
     import torch
 
@@ -756,13 +803,14 @@ def run_serving(args) -> None:
     _warm_server_kernels(capi, precision)
     calib = serving_requests(args.serving_requests, args.seed, capi)
     log(f"serving: {len(calib)} calibration requests, {sum(len(r['y0']) for r in calib)} particles")
-    _serial(capi, calib, cap, precision)  # warm: grows the host path's buffers, as the server's pool is warmed
-    t_serial, acc_serial, alone = _serial(capi, calib, cap, precision)
+    slots = ResultSlots(args.result_buffers, cap)
+    _serial(capi, calib, cap, precision, slots)  # warm, as the server's pool is warmed
+    t_serial, acc_serial, alone = _serial(capi, calib, cap, precision, slots)
     log(f"serving: serial {t_serial:.2f} s")
     gpu = gpu_uuid(torch, torch.device(f"cuda:{local}"))
     with Server(memory_fraction=0.6, streams=args.streams, sm_reserve_percent=args.sm_reserve) as srv:
-        _serve(srv, calib, cap, precision, open_loop=False)
-        sat = sorted((_serve(srv, calib, cap, precision, open_loop=False) for _ in range(3)), key=lambda p: p[0])
+        _serve(srv, calib, cap, precision, False, slots)
+        sat = sorted((_serve(srv, calib, cap, precision, False, slots) for _ in range(3)), key=lambda p: p[0])
         t_sat, acc_sat = sat[1][0], sat[1][1]
         capacity = len(calib) / t_sat
         log(f"serving: saturated {t_sat:.2f} s ({capacity:.2f} requests/s)")
@@ -772,16 +820,19 @@ def run_serving(args) -> None:
                 rate = load * capacity
                 count = max(8, int(round(rate * args.stream_seconds)))
                 stream = serving_requests(count, args.seed + 100 + k, capi, arrival_rate=rate)
-                t_run, acc_run, lat, capped = _serve(srv, stream, cap, precision, open_loop=True)
+                t_run, acc_run, lat, capped, waits = _serve(srv, stream, cap, precision, True, slots)
                 pct = _pct(lat)
                 sweeps.append({"offered_load": load, "rate_per_s": rate, "requests": count,
                                "particles": int(sum(len(r["y0"]) for r in stream)),
                                "arrival_window_s": float(stream[-1]["at"]), "seconds": t_run,
                                "accepted_steps_per_s": acc_run / t_run, "latency_ms": pct,
-                               "capped_requests": capped, "capped_fraction": capped / count})
+                               "capped_requests": capped, "capped_fraction": capped / count,
+                               "client_buffer_wait_ms_p99": float(np.percentile(np.array(waits) * 1e3, 99))
+                               if waits else 0.0})
                 log(f"serving: load {load} ({rate:.2f}/s, {count} requests) p50 {pct['p50']:.1f} ms "
                     f"p99 {pct['p99']:.1f} ms")
         st = srv.stats()
+    slots.close()
     alone_ms = np.array(alone) * 1e3
     line = {
         "metric": "accepted steps/s (served request stream)",
@@ -798,7 +849,8 @@ def run_serving(args) -> None:
         "data": "synthetic (seeded request streams)",
         "config": {"workload": "serving", "calibration_requests": len(calib), "streams": args.streams,
                    "sm_reserve_percent": args.sm_reserve, "precision": args.precision,
-                   "trajectory_cap_bytes": cap, "stream_seconds": args.stream_seconds, "seed": args.seed},
+                   "trajectory_cap_bytes": cap, "result_buffers": args.result_buffers,
+                   "stream_seconds": args.stream_seconds, "seed": args.seed},
         "vs_serial": (acc_sat / t_sat) / (acc_serial / t_serial),
         "serial_plain": {"value": acc_serial / t_serial, "seconds": t_serial,
                          "latency_alone_ms": {"p50": float(np.percentile(alone_ms, 50)),
@@ -967,6 +1019,8 @@ def main() -> None:
     ap.add_argument("--trajectory-cap-mib", type=int, default=2048,
                     help="serving: largest trajectory returned to host memory; larger requests return final "
                          "states only")
+    ap.add_argument("--result-buffers", type=int, default=12,
+                    help="serving: page-locked result buffers of --trajectory-cap-mib each, reused across requests")
     ap.add_argument("--seed", type=int, default=4)
     args = ap.parse_args()
     if args.no_e2e:
