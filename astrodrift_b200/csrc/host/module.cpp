@@ -143,9 +143,9 @@ Tolerance extract_tolerance(const py::handle &obj)
     throw py::value_error("Expected (rtol, atol) tuple or single float tolerance value");
 }
 
-// validate_configuration (src/integrators/mod.rs:23-36).  The B200 build
+// validate_configuration (src/integrators/mod.rs:23-36).  This package
 // integrates on the GPU only; the reference's CPU engine is its own
-// line-by-line host port, which this build keeps as a test oracle rather
+// line-by-line host port, which this package keeps as a test oracle rather
 // than as a product path.
 void validate_configuration(const Config &c)
 {

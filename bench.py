@@ -232,7 +232,7 @@ def cpu_oracle_rate(workload: str, y0, ts, t_end, nt, sample: int, threads: int,
 
 def accuracy_vs_oracle(workload: str, y0, ts, t_end, nt, out_sample, accepted_sample, idx) -> dict:
     """Max relative error per sample and accepted-step agreement of a seeded
-    particle sample against the CPU oracle (the checker; run after timing).
+    particle sample against the CPU oracle (run after timing).
     out_sample: (nt, len(idx), 6) of the benchmarked build."""
     oracle = _oracle()
     wl = WORKLOADS[workload]
@@ -637,7 +637,7 @@ def serving_requests(count, seed, capi, arrival_rate=None):
 class ResultSlots:
     """Page-locked result buffers of cap_bytes each (drift_host_alloc), reused
     across requests, as a serving client keeps them: results then copy at the
-    device-to-host rate instead of through the driver's pageable staging and
+    device-to-host rate instead of through the CUDA driver's pageable staging and
     first-touch page faults."""
 
     def __init__(self, count: int, cap_bytes: int):

@@ -1,8 +1,8 @@
-"""``drift``: the reference's import name for this build.
+"""``drift``: the reference's import name for astrodrift_b200.
 
 lbparticles/astrodrift is imported as ``import drift as dft`` with the native
 module at ``drift.drift_rs`` (python/drift/__init__.py).  This package gives
-this build the same two names, so host code and tests written against the
+astrodrift_b200 the same two names, so host code and tests written against the
 reference import it unchanged:
 
     import drift as dft

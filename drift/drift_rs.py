@@ -1,7 +1,7 @@
 """``drift.drift_rs``: the native module under the reference's name.
 
 The reference's ``drift.drift_rs`` is its compiled extension
-(python/drift/drift_rs.pyi).  Here it is this build's pybind11 host module,
+(python/drift/drift_rs.pyi).  Here it is astrodrift_b200's pybind11 host module,
 ``astrodrift_b200._drift``, which serves the same names.
 """
 

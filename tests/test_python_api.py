@@ -2,7 +2,7 @@
 
 Follows the reference's Python tests (tests/test_python_containers.py,
 test_python_selectors.py, test_python_time_grids.py, test_python_errors.py
-and the host-only parts of test_python_smoke.py) with this build's
+and the host-only parts of test_python_smoke.py) with this package's
 deliberate differences: particle and output-time caps are lifted
 (2^30 particles, 2^24 times) and the engine is the GPU.
 """
@@ -220,7 +220,7 @@ def test_unimplemented_integrator_is_rejected_before_execution(engine, method, i
 
 
 def test_cpu_engine_is_not_a_product_path() -> None:
-    # The reference's CPU engine is its host port; this build keeps that port
+    # The reference's CPU engine is its host port; this package keeps that port
     # as the test oracle and integrates on the GPU only.
     with pytest.raises(NotImplementedError, match=r"CPU \+ GALPY DOP853 is not implemented"):
         dft.Config(engine=dft.Engine.CPU, method=dft.Method.DOP853)

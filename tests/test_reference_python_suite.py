@@ -1,8 +1,8 @@
-"""The reference's own Python tests, run unchanged against this build.
+"""The reference's own Python tests, run unchanged against astrodrift_b200.
 
 lbparticles/astrodrift tests its Python surface with ``import drift as dft``
 (tests/test_python_{containers,selectors,time_grids,errors}.py).  The
-``drift`` package of this repository gives that name to this build, so those
+``drift`` package of this repository gives that name to astrodrift_b200, so those
 files run here as they are, from the reference's checkout when one is present
 on this machine (the test is skipped otherwise; it needs no GPU).  Every test
 must pass except the listed differences, each of which is a deliberate
@@ -33,7 +33,7 @@ EXPECTED_DIFFERENCES = {
     ("test_python_time_grids", "test_invalid_time_grids_are_rejected", "between 2 and 1024"):
         "the 1,024-output cap is raised to 2^24 (the message names the new bound)",
     ("test_python_errors", "test_failed_integration_raises_drift_integration_error", None):
-        "its Config uses Engine.CPU; the reference's CPU engine is this build's test oracle, "
+        "its Config uses Engine.CPU; the reference's CPU engine is this package's test oracle, "
         "not a product path, and raises NotImplementedError",
 }
 
@@ -78,8 +78,8 @@ def test_reference_python_tests_pass_except_listed_differences(tmp_path):
         assert any(c == file and (n == func or n.startswith(func + "[")) for c, n in expected), func
 
 
-def test_drift_name_is_this_build():
-    """``import drift`` and ``drift.drift_rs`` serve this build's classes."""
+def test_drift_name_serves_astrodrift_b200():
+    """``import drift`` and ``drift.drift_rs`` serve astrodrift_b200's classes."""
     code = (
         "import drift as dft, drift.drift_rs as rs, astrodrift_b200 as ab\n"
         "assert dft.Config is ab.Config is rs.Config\n"

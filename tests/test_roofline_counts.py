@@ -22,7 +22,7 @@ def test_committed_counts_match_a_fresh_count():
     for name, r in rows.items():
         assert roofline_counts.fit(r) == committed[name], name  # fit() raises unless exact
     plummer = committed["dop853_plummer"]["flops"]
-    # the survey's hand count for DOP853 + Plummer was about 2,065 per accepted step
+    # counting the reference's DOP853 step and Plummer force by hand gives about 2,065 per accepted step
     assert abs(plummer["per_accepted"] - 2065) < 50
     assert committed["dop853_plummer"]["pow"]["per_accepted"] == 17  # 15 forces + 2 controller pows
 
