@@ -60,6 +60,7 @@ EXPORTED = (
     "drift_server_create",
     "drift_server_submit",
     "drift_server_wait",
+    "drift_server_wait_any",
     "drift_server_stats_get",
     "drift_server_cancel",
     "drift_server_destroy",

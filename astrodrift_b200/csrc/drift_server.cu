@@ -541,6 +541,41 @@ int drift_server_wait(drift_server *s, uint64_t ticket, double timeout_s, int *r
     return DRIFT_SUCCESS;
 }
 
+int drift_server_wait_any(drift_server *s, const uint64_t *tickets, int32_t count, double timeout_s,
+                          int32_t *index, int *request_result, double *latency_s)
+{
+    if (!s || !tickets || !index || count < 1)
+        return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument or empty ticket list");
+    std::unique_lock<std::mutex> lock(s->mu);
+    std::vector<Request *> rs((size_t)count);
+    for (int32_t i = 0; i < count; i++) {
+        auto it = s->requests.find(tickets[i]);
+        if (it == s->requests.end())
+            return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown ticket");
+        rs[i] = it->second.get();
+    }
+    // The earliest completion among the finished requests, so that a client
+    // retiring one request at a time sees them in completion order.
+    int32_t found = -1;
+    auto pred = [&] {
+        for (int32_t i = 0; i < count; i++)
+            if (rs[i]->done && (found < 0 || rs[i]->completed < rs[found]->completed)) found = i;
+        return found >= 0;
+    };
+    if (timeout_s > 0) {
+        if (!s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s), pred))
+            return drift_internal_fail(DRIFT_ERROR_TIMEOUT, "every request still running");
+    } else {
+        s->cv_done.wait(lock, pred);
+    }
+    Request *r = rs[found];
+    *index = found;
+    if (request_result) *request_result = r->result;
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->completed - r->submitted).count();
+    s->requests.erase(r->ticket);
+    return DRIFT_SUCCESS;
+}
+
 int drift_server_stats_get(drift_server *s, drift_server_stats *out)
 {
     if (!s || !out) return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument");

@@ -47,6 +47,9 @@ def _lib():
         L.drift_server_wait.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_double,
                                         ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
         L.drift_server_stats_get.argtypes = [ctypes.c_void_p, ctypes.POINTER(ServerStats)]
+        L.drift_server_wait_any.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int32,
+                                            ctypes.c_double, ctypes.POINTER(ctypes.c_int32),
+                                            ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
         L.drift_server_cancel.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
         L.drift_server_destroy.argtypes = [ctypes.c_void_p]
         L._server_bound = True
@@ -103,14 +106,17 @@ class Request:
         latency = ctypes.c_double(0.0)
         capi.check(_lib().drift_server_wait(self.server._ptr, self.ticket, timeout, ctypes.byref(result),
                                             ctypes.byref(latency)), "drift_server_wait")
-        if result.value == 7:  # DRIFT_ERROR_CANCELLED
-            self._keep = None
-            raise RequestCancelled("request cancelled")
-        if result.value != 0:
-            raise RuntimeError(f"request failed: {capi.lib().drift_result_string(result.value).decode()}")
-        out = dict(self.arrays)
-        out["latency_s"] = latency.value
+        return self._finish(result.value, latency.value)
+
+    def _finish(self, result: int, latency: float) -> dict:
+        # the ticket has been released: results or the request's error
         self._keep = None
+        if result == 7:  # DRIFT_ERROR_CANCELLED
+            raise RequestCancelled("request cancelled")
+        if result != 0:
+            raise RuntimeError(f"request failed: {capi.lib().drift_result_string(result).decode()}")
+        out = dict(self.arrays)
+        out["latency_s"] = latency
         return out
 
 
@@ -169,6 +175,21 @@ class Server:
         capi.check(_lib().drift_server_submit(self._ptr, ctypes.byref(L), ctypes.byref(ticket)),
                    "drift_server_submit")
         return Request(self, ticket.value, (y0, ts, t_end, L, pinned), arrays)
+
+    def wait_any(self, requests, timeout: float = 0.0) -> tuple[int, dict]:
+        """Block until any of ``requests`` completes (drift_server_wait_any)
+        and return (its index in ``requests``, its results).  The others stay
+        pending and can be waited for again.  ``timeout`` as Request.wait; a
+        failed or cancelled request raises as Request.wait does."""
+        if not self._ptr:
+            raise RuntimeError("the server is closed")
+        requests = list(requests)
+        tickets = (ctypes.c_uint64 * len(requests))(*[r.ticket for r in requests])
+        index, result, latency = ctypes.c_int32(-1), ctypes.c_int(0), ctypes.c_double(0.0)
+        capi.check(_lib().drift_server_wait_any(self._ptr, tickets, len(requests), timeout, ctypes.byref(index),
+                                                ctypes.byref(result), ctypes.byref(latency)),
+                   "drift_server_wait_any")
+        return index.value, requests[index.value]._finish(result.value, latency.value)
 
     def stats(self) -> dict:
         st = ServerStats()

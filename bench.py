@@ -658,17 +658,17 @@ def _serve(srv, reqs, cap_bytes, precision, open_loop: bool, slots: ResultSlots)
     """Submit every request (at its arrival time when open_loop, else all at
     once); returns (seconds, accepted steps, latencies s, capped count, client
     waits s).  Results come back into the page-locked slots; when all are in
-    use the client first waits for its oldest request (the wait is recorded;
-    the request's own latency runs from its submission).  A request whose
-    trajectory exceeds cap_bytes returns its final states only (its
-    integration, dense output included, is unchanged; the samples are not
-    stored)."""
+    use the client first waits for whichever request in flight finishes first
+    (drift_server_wait_any; the wait is recorded, the request's own latency
+    runs from its submission).  A request whose trajectory exceeds cap_bytes
+    returns its final states only (its integration, dense output included, is
+    unchanged; the samples are not stored)."""
     inflight, lat, waits, capped, acc = [], [], [], 0, 0
 
     def retire():
         nonlocal acc
-        h, slot = inflight.pop(0)
-        res = h.wait(timeout=3600.0)
+        i, res = srv.wait_any([h for h, _ in inflight], timeout=3600.0)
+        _, slot = inflight.pop(i)
         lat.append(res["latency_s"])
         acc += int(res["accepted"].astype(np.int64).sum())
         if slot is not None:

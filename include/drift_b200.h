@@ -493,6 +493,14 @@ int drift_server_submit(drift_server *server, const drift_launch *request, uint6
  * latency_s the time from submission to completion.  Releases the ticket. */
 int drift_server_wait(drift_server *server, uint64_t ticket, double timeout_s, int *request_result,
                       double *latency_s);
+/* Blocks until any of `count` requests completes (timeout_s as above) and
+ * releases that one ticket: *index receives its position in `tickets` (the
+ * earliest completion when several have finished), request_result and
+ * latency_s as drift_server_wait.  The other tickets stay valid.  A client
+ * holding a fixed set of result buffers retires whichever request finishes
+ * first instead of the oldest one. */
+int drift_server_wait_any(drift_server *server, const uint64_t *tickets, int32_t count, double timeout_s,
+                          int32_t *index, int *request_result, double *latency_s);
 int drift_server_stats_get(drift_server *server, drift_server_stats *stats);
 /* Cancels one request: none of its particles that are not yet on the GPU
  * will run.  Particles already admitted finish (their results are written

@@ -197,6 +197,17 @@ def test_context_entry_points_validate_their_arguments():
     assert lib.drift_context_destroy(None) == 0
 
 
+def test_server_entry_points_validate_their_arguments():
+    lib = serving._lib()
+    tickets = (ctypes.c_uint64 * 1)(1)
+    index = ctypes.c_int32(-1)
+    assert lib.drift_server_wait_any(None, tickets, 1, 0.0, ctypes.byref(index), None, None) == INVALID_ARGUMENT
+    assert "empty ticket list" in lib.drift_last_error().decode()
+    assert lib.drift_server_wait(None, 1, 0.0, None, None) == INVALID_ARGUMENT
+    assert lib.drift_server_cancel(None, 1) == INVALID_ARGUMENT
+    assert lib.drift_server_destroy(None) == 0
+
+
 def test_tuning_choices_persist_in_a_json_file(tmp_path, monkeypatch):
     import json
 

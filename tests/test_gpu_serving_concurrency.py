@@ -9,6 +9,8 @@
   keeps serving.
 * The host path (drift_integrate_host, whose buffer growth frees device
   memory) runs to completion while a server batch is in flight.
+* drift_server_wait_any hands back whichever request finishes first: small
+  requests submitted after a large one are retired before it.
 Every wait here has a time limit, so a stall fails the test instead of
 holding the run.
 """
@@ -125,3 +127,33 @@ def test_host_path_runs_while_a_server_batch_is_in_flight(cuda_device):
             assert (res["status"] == 0).all()
         out = h.wait(timeout=WAIT_S)
     assert (out["status"] == 0).all()
+
+
+def test_wait_any_retires_requests_in_completion_order(cuda_device):
+    n = 60_000
+    with Server(streams=4, memory_fraction=0.5) as srv:
+        large = srv.submit(capi.DOP853, capi.bovy(), _disc(n, 7), t_end=np.full(n, 1500.0), nt=101,
+                           rtol=1e-11, atol=1e-11, precision=capi.FMA)
+        pending, inputs = [large], {}
+        for i in range(8):
+            kw = _small(200 + i)
+            h = srv.submit(kw["method"], kw["pot"], kw["y0"], ts=kw["ts"], rtol=kw["rtol"], atol=kw["atol"])
+            pending.append(h)
+            inputs[h.ticket] = kw
+        retired = []
+        while pending:
+            i, res = srv.wait_any(pending, timeout=WAIT_S)
+            h = pending.pop(i)
+            retired.append(h)
+            if h is large:
+                assert (res["status"] == 0).all()
+                continue
+            kw = inputs[h.ticket]
+            ref = capi.integrate_host(kw["method"], kw["pot"], kw["y0"], ts=kw["ts"], rtol=kw["rtol"],
+                                      atol=kw["atol"], schedule=capi.PLAIN)
+            np.testing.assert_array_equal(res["out"], ref["out"])
+        # the small requests submitted after the large one are retired before it
+        assert retired[-1] is large
+        # a retired ticket is released: waiting for it again is an error
+        with pytest.raises(RuntimeError, match="unknown ticket"):
+            srv.wait_any([large], timeout=1.0)
