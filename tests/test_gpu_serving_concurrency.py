@@ -42,7 +42,22 @@ def _small(seed):
                 ts=np.linspace(0.0, 10.0, 11), rtol=1e-10, atol=1e-10)
 
 
-def test_small_requests_finish_while_a_large_pageable_request_runs(cuda_device):
+@pytest.fixture(scope="module")
+def warm(cuda_device):
+    """Launches the kernels these tests time once, small, before any of them
+    runs: a kernel's first launch in a process loads its code (lazy module
+    loading), which waits for the device, so a first small batch launched
+    beside a running large one would measure that wait instead of serving."""
+    kw = _small(0)
+    for schedule in (capi.PLAIN, capi.ORDERED):
+        capi.integrate_host(kw["method"], kw["pot"], kw["y0"], ts=kw["ts"], rtol=kw["rtol"], atol=kw["atol"],
+                            schedule=schedule)
+        capi.integrate_host(capi.DOP853, capi.bovy(), _disc(64, 1), t_end=np.full(64, 1.0), nt=3, rtol=1e-11,
+                            atol=1e-11, precision=capi.FMA, schedule=schedule)
+    return cuda_device
+
+
+def test_small_requests_finish_while_a_large_pageable_request_runs(warm):
     n = 60_000
     y0 = _disc(n, 1)
     t_end = np.full(n, 1500.0)
@@ -129,7 +144,7 @@ def test_host_path_runs_while_a_server_batch_is_in_flight(cuda_device):
     assert (out["status"] == 0).all()
 
 
-def test_wait_any_retires_requests_in_completion_order(cuda_device):
+def test_wait_any_retires_requests_in_completion_order(warm):
     n = 60_000
     with Server(streams=4, memory_fraction=0.5) as srv:
         large = srv.submit(capi.DOP853, capi.bovy(), _disc(n, 7), t_end=np.full(n, 1500.0), nt=101,
