@@ -144,6 +144,8 @@ struct drift_server {
     std::mutex mu;
     std::condition_variable cv_work;  // scheduler wake-up
     std::condition_variable cv_done;  // waiters
+    std::condition_variable cv_idle;  // destroy: the last waiter has left
+    int waiters = 0;                  // threads inside drift_server_wait(_any)
     std::deque<Request *> pending;
     std::map<uint64_t, std::unique_ptr<Request>> requests;
     size_t bytes_inflight = 0;
@@ -412,6 +414,18 @@ struct drift_server {
     }
 };
 
+// Counts a thread inside a wait for drift_server_destroy, which frees the
+// server only once every waiter has left.  Constructed after the wait's lock
+// and so destroyed while it is still held.
+struct WaiterScope {
+    drift_server *s;
+    explicit WaiterScope(drift_server *srv) : s(srv) { s->waiters++; }
+    ~WaiterScope()
+    {
+        if (--s->waiters == 0) s->cv_idle.notify_all();
+    }
+};
+
 extern "C" {
 
 int drift_server_create(const drift_server_options *options, drift_server **out)
@@ -524,6 +538,7 @@ int drift_server_wait(drift_server *s, uint64_t ticket, double timeout_s, int *r
 {
     if (!s) return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "server is NULL");
     std::unique_lock<std::mutex> lock(s->mu);
+    WaiterScope scope(s);
     auto it = s->requests.find(ticket);
     if (it == s->requests.end())
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "unknown ticket");
@@ -547,6 +562,7 @@ int drift_server_wait_any(drift_server *s, const uint64_t *tickets, int32_t coun
     if (!s || !tickets || !index || count < 1)
         return drift_internal_fail(DRIFT_ERROR_INVALID_ARGUMENT, "NULL argument or empty ticket list");
     std::unique_lock<std::mutex> lock(s->mu);
+    WaiterScope scope(s);
     std::vector<Request *> rs((size_t)count);
     for (int32_t i = 0; i < count; i++) {
         auto it = s->requests.find(tickets[i]);
@@ -630,6 +646,12 @@ int drift_server_destroy(drift_server *s)
     }
     for (auto &w : s->workers)
         if (w->thread.joinable()) w->thread.join();
+    {
+        // Every request has ended (cancelled, or its batches finished), so
+        // each thread still inside a wait is on its way out.
+        std::unique_lock<std::mutex> lock(s->mu);
+        s->cv_idle.wait(lock, [s] { return s->waiters == 0; });
+    }
     for (auto st : s->streams) {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);

@@ -11,7 +11,9 @@ overlap the integration of other requests.
 
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import threading
 
 import numpy as np
 
@@ -92,24 +94,23 @@ class Request:
         """Stop admitting this request's particles (drift_server_cancel);
         wait() then raises RequestCancelled once the particles already on the
         GPU have finished."""
-        if not self.server._ptr:
-            raise RuntimeError("the server is closed")
-        capi.check(_lib().drift_server_cancel(self.server._ptr, self.ticket), "drift_server_cancel")
+        with self.server._call() as ptr:
+            capi.check(_lib().drift_server_cancel(ptr, self.ticket), "drift_server_cancel")
 
     def wait(self, timeout: float = 0.0) -> dict:
         """Block until the request completes; ``timeout`` > 0 bounds the wait
         (RuntimeError with the library's timeout message when it runs out;
         the request stays valid and can be waited for again)."""
-        if not self.server._ptr:
-            raise RuntimeError("the server is closed")
         result = ctypes.c_int(0)
         latency = ctypes.c_double(0.0)
-        capi.check(_lib().drift_server_wait(self.server._ptr, self.ticket, timeout, ctypes.byref(result),
-                                            ctypes.byref(latency)), "drift_server_wait")
+        with self.server._call() as ptr:
+            capi.check(_lib().drift_server_wait(ptr, self.ticket, timeout, ctypes.byref(result),
+                                                ctypes.byref(latency)), "drift_server_wait")
         return self._finish(result.value, latency.value)
 
     def _finish(self, result: int, latency: float) -> dict:
         # the ticket has been released: results or the request's error
+        self.server._released(self.ticket)
         self._keep = None
         if result == 7:  # DRIFT_ERROR_CANCELLED
             raise RequestCancelled("request cancelled")
@@ -134,9 +135,33 @@ class Server:
                              select_device=int(device is not None),
                              device=int(device) if device is not None else 0)
         self._ptr = ctypes.c_void_p()
+        # Calls in progress and tickets not yet waited for: close() cancels
+        # the tickets and lets every call return before freeing the server.
+        self._cond = threading.Condition()
+        self._calls = 0
+        self._closing = False
+        self._tickets: set[int] = set()
         capi.check(_lib().drift_server_create(ctypes.byref(opts), ctypes.byref(self._ptr)),
                    "drift_server_create")
         self.device_index = self.stats()["device"]
+
+    @contextlib.contextmanager
+    def _call(self):
+        """The server pointer for one C call, which close() waits for."""
+        with self._cond:
+            if not self._ptr or self._closing:
+                raise RuntimeError("the server is closed")
+            self._calls += 1
+        try:
+            yield self._ptr
+        finally:
+            with self._cond:
+                self._calls -= 1
+                self._cond.notify_all()
+
+    def _released(self, ticket: int) -> None:
+        with self._cond:
+            self._tickets.discard(ticket)
 
     def submit(self, method, pot, y0, *, ts=None, t_end=None, nt=None, t0=0.0, rtol=1e-12,
                atol=1e-12, precision=capi.EXACT, schedule=capi.ORDERED, out=None,
@@ -172,8 +197,11 @@ class Server:
         L.status, L.err_code = arrays["status"].ctypes.data, arrays["err"].ctypes.data
         L.n_accepted, L.n_rejected = arrays["accepted"].ctypes.data, arrays["rejected"].ctypes.data
         ticket = ctypes.c_uint64(0)
-        capi.check(_lib().drift_server_submit(self._ptr, ctypes.byref(L), ctypes.byref(ticket)),
-                   "drift_server_submit")
+        with self._call() as ptr:
+            capi.check(_lib().drift_server_submit(ptr, ctypes.byref(L), ctypes.byref(ticket)),
+                       "drift_server_submit")
+            with self._cond:
+                self._tickets.add(ticket.value)
         return Request(self, ticket.value, (y0, ts, t_end, L, pinned), arrays)
 
     def wait_any(self, requests, timeout: float = 0.0) -> tuple[int, dict]:
@@ -181,24 +209,38 @@ class Server:
         and return (its index in ``requests``, its results).  The others stay
         pending and can be waited for again.  ``timeout`` as Request.wait; a
         failed or cancelled request raises as Request.wait does."""
-        if not self._ptr:
-            raise RuntimeError("the server is closed")
         requests = list(requests)
         tickets = (ctypes.c_uint64 * len(requests))(*[r.ticket for r in requests])
         index, result, latency = ctypes.c_int32(-1), ctypes.c_int(0), ctypes.c_double(0.0)
-        capi.check(_lib().drift_server_wait_any(self._ptr, tickets, len(requests), timeout, ctypes.byref(index),
-                                                ctypes.byref(result), ctypes.byref(latency)),
-                   "drift_server_wait_any")
+        with self._call() as ptr:
+            capi.check(_lib().drift_server_wait_any(ptr, tickets, len(requests), timeout, ctypes.byref(index),
+                                                    ctypes.byref(result), ctypes.byref(latency)),
+                       "drift_server_wait_any")
         return index.value, requests[index.value]._finish(result.value, latency.value)
 
     def stats(self) -> dict:
         st = ServerStats()
-        capi.check(_lib().drift_server_stats_get(self._ptr, ctypes.byref(st)), "drift_server_stats_get")
+        with self._call() as ptr:
+            capi.check(_lib().drift_server_stats_get(ptr, ctypes.byref(st)), "drift_server_stats_get")
         return {name: getattr(st, name) for name, _ in ServerStats._fields_}
 
     def close(self):
-        if self._ptr:
-            _lib().drift_server_destroy(self._ptr)
+        """Cancels the requests not yet waited for (drift_server_cancel: those
+        with particles on the GPU finish them), lets every call in progress on
+        other threads return (their waits end with the result or
+        RequestCancelled), then destroys the server.  Later calls raise."""
+        with self._cond:
+            if not self._ptr or self._closing:
+                return
+            self._closing = True
+            tickets = sorted(self._tickets)
+            ptr = self._ptr
+        for t in tickets:
+            _lib().drift_server_cancel(ptr, t)  # a ticket released meanwhile only reports an error
+        with self._cond:
+            self._cond.wait_for(lambda: self._calls == 0)
+        _lib().drift_server_destroy(ptr)
+        with self._cond:
             self._ptr = ctypes.c_void_p()
 
     def __enter__(self):

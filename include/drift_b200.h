@@ -510,7 +510,10 @@ int drift_server_stats_get(drift_server *server, drift_server_stats *stats);
  * finished changes nothing.  The ticket stays valid until waited for. */
 int drift_server_cancel(drift_server *server, uint64_t ticket);
 /* Cancels pending requests (their waiters receive DRIFT_ERROR_CANCELLED),
- * finishes the batches in flight and frees the server. */
+ * finishes the batches in flight and frees the server.  Waits already in
+ * progress on other threads return (their request's result, or
+ * DRIFT_ERROR_CANCELLED) before the server is freed; no call on the server
+ * may begin once destroy has been called. */
 int drift_server_destroy(drift_server *server);
 
 /* The reference kernel signatures (kernels/src/lib.rs:143-173, 188-216):

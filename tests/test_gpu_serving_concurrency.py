@@ -11,16 +11,24 @@
   memory) runs to completion while a server batch is in flight.
 * drift_server_wait_any hands back whichever request finishes first: small
   requests submitted after a large one are retired before it.
+* Destroying a server while another thread waits: drift_server_destroy lets
+  the thread inside drift_server_wait return before it frees the server, and
+  Server.close() cancels what other threads wait for and lets their calls
+  return first.
 Every wait here has a time limit, so a stall fails the test instead of
 holding the run.
 """
 
 from __future__ import annotations
 
+import ctypes
+import threading
+import time
+
 import numpy as np
 import pytest
 
-from astrodrift_b200 import capi
+from astrodrift_b200 import capi, serving
 from astrodrift_b200.serving import RequestCancelled, Server
 
 pytestmark = pytest.mark.gpu
@@ -172,3 +180,62 @@ def test_wait_any_retires_requests_in_completion_order(warm):
         # a retired ticket is released: waiting for it again is an error
         with pytest.raises(RuntimeError, match="unknown ticket"):
             srv.wait_any([large], timeout=1.0)
+
+
+def _one_stream_with_a_queued_request():
+    """A server whose only stream runs a long Bovy request, with a small
+    request queued behind it."""
+    srv = Server(streams=1, memory_fraction=0.3)
+    n = 20_000
+    srv.submit(capi.DOP853, capi.bovy(), _disc(n, 3), t_end=np.full(n, 400.0), nt=11, rtol=1e-10, atol=1e-10,
+               precision=capi.FMA)
+    kw = _small(300)
+    queued = srv.submit(kw["method"], kw["pot"], kw["y0"], ts=kw["ts"], rtol=kw["rtol"], atol=kw["atol"])
+    return srv, queued
+
+
+def test_destroy_lets_a_thread_inside_a_wait_return_first(warm):
+    srv, queued = _one_stream_with_a_queued_request()
+    ptr, lib = srv._ptr, serving._lib()
+    got = {}
+
+    def raw_wait():
+        result, latency = ctypes.c_int(-1), ctypes.c_double(0.0)
+        got["rc"] = lib.drift_server_wait(ptr, queued.ticket, WAIT_S, ctypes.byref(result), ctypes.byref(latency))
+        got["result"] = result.value
+
+    t = threading.Thread(target=raw_wait)
+    t.start()
+    time.sleep(0.3)  # the thread is blocked inside drift_server_wait
+    assert lib.drift_server_destroy(ptr) == 0
+    t.join(timeout=WAIT_S)
+    assert not t.is_alive()
+    srv._ptr = ctypes.c_void_p()  # destroyed above, not through the handle
+    assert got["rc"] == 0
+    assert got["result"] in (0, 7)  # finished, or DRIFT_ERROR_CANCELLED while queued
+
+
+def test_close_cancels_what_other_threads_wait_for(warm):
+    srv, queued = _one_stream_with_a_queued_request()
+    outcome = {}
+
+    def waiter():
+        try:
+            outcome["res"] = queued.wait(timeout=WAIT_S)
+        except RequestCancelled:
+            outcome["cancelled"] = True
+        except Exception as e:  # noqa: BLE001 - reported below
+            outcome["error"] = repr(e)
+
+    t = threading.Thread(target=waiter)
+    t.start()
+    deadline = time.monotonic() + 10.0
+    while srv._calls == 0 and time.monotonic() < deadline:
+        time.sleep(0.001)  # until the waiter's call is in progress
+    srv.close()
+    t.join(timeout=WAIT_S)
+    assert not t.is_alive()
+    assert "error" not in outcome, outcome
+    assert outcome.get("cancelled") or (outcome["res"]["status"] == 0).all()
+    with pytest.raises(RuntimeError, match="closed"):
+        srv.stats()
