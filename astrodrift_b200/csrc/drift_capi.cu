@@ -1033,10 +1033,26 @@ int drift_integrate_host(const drift_launch *L)
 }  // extern "C"
 
 // The host path on a given context (its device current, the launch valid).
+static int host_integrate_locked(DeviceContext *ctx, const drift_launch *L);
+
 static int host_integrate(DeviceContext *ctx, const drift_launch *L)
 {
-    int rc = DRIFT_SUCCESS;
     std::lock_guard<std::mutex> lock(ctx->mu);
+    const int rc = host_integrate_locked(ctx, L);
+    if (rc != DRIFT_SUCCESS) {
+        // An error can leave the launch and copies into the caller's buffers
+        // in flight: they end before the caller sees the error (and may free
+        // those buffers).  A device fault makes these waits return at once.
+        for (cudaStream_t st : {ctx->streams[0], ctx->streams[1], ctx->poll_stream})
+            if (st) cudaStreamSynchronize(st);
+        cudaGetLastError();
+    }
+    return rc;
+}
+
+static int host_integrate_locked(DeviceContext *ctx, const drift_launch *L)
+{
+    int rc = DRIFT_SUCCESS;
     drift::TraceRange trace("drift host integrate");
 
     const int64_t n = L->n;
