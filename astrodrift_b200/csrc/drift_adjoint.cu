@@ -296,8 +296,12 @@ __device__ __forceinline__ void recompute_step(const Pot &pot, const double *y, 
     }
 }
 
+#ifndef DRIFT_ADJ_MIN_BLOCKS
+#define DRIFT_ADJ_MIN_BLOCKS 1
+#endif
+
 template <class Pot, class Jac>
-__global__ void __launch_bounds__(ADJ_THREADS) adjoint_kernel(const __grid_constant__ AdjointArgs a)
+__global__ void __launch_bounds__(ADJ_THREADS, DRIFT_ADJ_MIN_BLOCKS) adjoint_kernel(const __grid_constant__ AdjointArgs a)
 {
     __shared__ __align__(16) double table[BOVY_SMEM_DOUBLES];
     if (std::is_same<Pot, Bovy>::value) {
