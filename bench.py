@@ -72,7 +72,9 @@ WORKLOADS = {
         potential="bovy composite (bulge alpha 1.8, rc 0.2375, F_r(1) -0.05; MN 0.7574802019, a 0.375, "
                   "b 0.035; NFW 4.852230533528, a 2)",
         grid="per-particle t0 = 0 .. t_end ~ U[10, 1000], 101 outputs", counts="dop853_bovy",
-        traffic_per_particle=None, traffic_source=None,
+        traffic_per_particle=(0.965953280e9 + 1.748899072e9) / 262144,
+        traffic_source="ncu dram__bytes_read+write of the first 262,144 particles "
+                       "(profiles/dop853_bovy_uneven_slices.txt, section 7), times particles",
         data="synthetic (seeded Bovy disc: R log-uniform [0.05, 20], z ~ N(0, 0.1 R), 10 % dispersion)"),
     "plummer": dict(
         name="plummer-dop853", particles=1 << 20, nt=201, tol=1e-12, method="DOP853",
