@@ -210,13 +210,22 @@ class Server:
         pending and can be waited for again.  ``timeout`` as Request.wait; a
         failed or cancelled request raises as Request.wait does."""
         requests = list(requests)
+        got = self._wait_any(requests, timeout, poll=False)
+        return got[0], requests[got[0]]._finish(got[1], got[2])
+
+    def _wait_any(self, requests, timeout: float, poll: bool):
+        """drift_server_wait_any over ``requests`` (all of this server):
+        (index, drift_result, latency), or None when ``poll`` and the timeout
+        ran out (otherwise that raises like any other error)."""
         tickets = (ctypes.c_uint64 * len(requests))(*[r.ticket for r in requests])
         index, result, latency = ctypes.c_int32(-1), ctypes.c_int(0), ctypes.c_double(0.0)
         with self._call() as ptr:
-            capi.check(_lib().drift_server_wait_any(ptr, tickets, len(requests), timeout, ctypes.byref(index),
-                                                    ctypes.byref(result), ctypes.byref(latency)),
-                       "drift_server_wait_any")
-        return index.value, requests[index.value]._finish(result.value, latency.value)
+            rc = _lib().drift_server_wait_any(ptr, tickets, len(requests), timeout, ctypes.byref(index),
+                                              ctypes.byref(result), ctypes.byref(latency))
+        if poll and rc == 6:  # DRIFT_ERROR_TIMEOUT: nothing finished yet
+            return None
+        capi.check(rc, "drift_server_wait_any")
+        return index.value, result.value, latency.value
 
     def stats(self) -> dict:
         st = ServerStats()
@@ -336,6 +345,33 @@ class Router:
 
     def stats(self) -> list[dict]:
         return [s.stats() for s in self.servers]
+
+    def wait_any(self, requests, timeout: float = 0.0, poll_s: float = 1e-3) -> tuple[int, dict]:
+        """Server.wait_any across servers: (index in ``requests``, results)
+        of the first request to finish.  Requests of one server wait in one
+        call; requests spread over several servers are polled, each server's
+        wait bounded by ``poll_s``, until one finishes or ``timeout`` (> 0)
+        runs out (RuntimeError)."""
+        import time
+
+        requests = list(requests)
+        if not requests:
+            raise ValueError("no requests to wait for")
+        groups: dict[int, list[int]] = {}
+        for i, r in enumerate(requests):
+            groups.setdefault(id(r.server), []).append(i)
+        if len(groups) == 1:
+            return requests[0].server.wait_any(requests, timeout)
+        deadline = time.monotonic() + timeout if timeout > 0 else None
+        while True:
+            for idx in groups.values():
+                server = requests[idx[0]].server
+                got = server._wait_any([requests[i] for i in idx], poll_s, poll=True)
+                if got is not None:
+                    i = idx[got[0]]
+                    return i, requests[i]._finish(got[1], got[2])
+            if deadline is not None and time.monotonic() > deadline:
+                raise RuntimeError("drift_server_wait_any: every request still running")
 
     def close(self):
         for s in self.servers:

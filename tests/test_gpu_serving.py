@@ -147,6 +147,31 @@ def test_router_sends_each_request_whole_to_the_freest_server(cuda_device):
         assert res["device"] == 0
 
 
+def test_router_wait_any_retires_requests_of_every_server(cuda_device):
+    """Router.wait_any over requests spread across two servers returns each
+    exactly once, with the result it gets alone."""
+    from astrodrift_b200.serving import Router
+
+    mix = _mix(seed=4, count=10)
+    servers = [Server(memory_bytes=64 << 20, streams=2), Server(memory_bytes=64 << 20, streams=2)]
+    with Router(servers) as rt:
+        pending, inputs = [], {}
+        for k, kw in enumerate(mix):  # alternately, so that both servers hold requests
+            args = {a: v for a, v in kw.items() if a not in ("method", "pot", "y0")}
+            h = servers[k % 2].submit(kw["method"], kw["pot"], kw["y0"], **args)
+            pending.append(h)
+            inputs[id(h)] = kw
+        done = 0
+        while pending:
+            i, res = rt.wait_any(pending, timeout=600)
+            h = pending.pop(i)
+            ref = _alone(inputs[id(h)])
+            np.testing.assert_array_equal(res["out"], ref["out"])
+            np.testing.assert_array_equal(res["status"], ref["status"])
+            done += 1
+    assert done == len(mix)
+
+
 def test_queued_bytes_match_the_host_estimate(cuda_device):
     from astrodrift_b200.serving import request_bytes
 

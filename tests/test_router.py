@@ -83,3 +83,52 @@ def test_router_spreads_requests_by_what_each_server_has_left():
 def test_router_needs_a_server():
     with pytest.raises(ValueError):
         Router([])
+
+
+class _PollingServer:
+    """Stands in for a Server in Router.wait_any: its requests finish after
+    a given number of polls."""
+
+    def __init__(self, finish_after):
+        self.finish_after = dict(finish_after)  # ticket -> polls before it is done
+        self.polls = 0
+
+    def _wait_any(self, requests, timeout, poll):
+        assert poll and timeout > 0
+        self.polls += 1
+        for i, r in enumerate(requests):
+            if self.polls >= self.finish_after[r.ticket]:
+                return i, 0, 0.25
+        return None
+
+    def wait_any(self, requests, timeout=0.0):
+        return 0, requests[0]._finish(0, 0.5)
+
+
+class _Req:
+    def __init__(self, server, ticket):
+        self.server, self.ticket = server, ticket
+
+    def _finish(self, result, latency):
+        return {"ticket": self.ticket, "result": result, "latency_s": latency}
+
+
+def test_router_wait_any_polls_every_server_until_one_request_finishes():
+    a, b = _PollingServer({1: 5, 2: 9}), _PollingServer({3: 3})
+    reqs = [_Req(a, 1), _Req(a, 2), _Req(b, 3)]
+    rt = Router([a, b])
+    i, res = rt.wait_any(reqs)
+    assert (i, res["ticket"]) == (2, 3)  # b's request finishes on its third poll
+    assert a.polls == 3 and b.polls == 3
+    # requests of one server wait in that server's own call
+    i, res = rt.wait_any([_Req(a, 1)])
+    assert (i, res["latency_s"]) == (0, 0.5)
+    with pytest.raises(ValueError):
+        rt.wait_any([])
+
+
+def test_router_wait_any_gives_up_at_its_timeout():
+    a, b = _PollingServer({1: 10**9}), _PollingServer({2: 10**9})
+    rt = Router([a, b])
+    with pytest.raises(RuntimeError, match="still running"):
+        rt.wait_any([_Req(a, 1), _Req(b, 2)], timeout=0.01)
