@@ -213,17 +213,6 @@ class Server:
         got = self._wait_any(requests, timeout, poll=False)
         return got[0], requests[got[0]]._finish(got[1], got[2])
 
-    def poll_any(self, requests, timeout: float):
-        """As wait_any, but returns None when none of ``requests`` finishes
-        within ``timeout`` (> 0) seconds: an event loop's non-blocking retire."""
-        if not timeout > 0:
-            raise ValueError("poll_any needs a timeout > 0")
-        requests = list(requests)
-        got = self._wait_any(requests, timeout, poll=True)
-        if got is None:
-            return None
-        return got[0], requests[got[0]]._finish(got[1], got[2])
-
     def _wait_any(self, requests, timeout: float, poll: bool):
         """drift_server_wait_any over ``requests`` (all of this server):
         (index, drift_result, latency), or None when ``poll`` and the timeout

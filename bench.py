@@ -656,75 +656,48 @@ class ResultSlots:
             b.free()
 
 
-def _serve(srv, reqs, cap_bytes, precision, open_loop: bool, slots):
+def _serve(srv, reqs, cap_bytes, precision, open_loop: bool, slots: ResultSlots):
     """Submit every request (at its arrival time when open_loop, else all at
     once); returns (seconds, accepted steps, latencies s, capped count, client
-    waits s).  Results come back into the page-locked slots.  A request that
-    needs a slot while all are in use waits, in arrival order, for the next
-    one to free up, without holding back later requests that need none; its
-    wait from arrival to submission is recorded, and its own latency runs
-    from its submission.  Finished requests are retired in completion order
-    (drift_server_wait_any).  A request whose trajectory exceeds cap_bytes
-    returns its final states only (its integration, dense output included,
-    is unchanged; the samples are not stored)."""
-    from collections import deque
-
+    waits s).  Results come back into the page-locked slots; when all are in
+    use the client first waits for whichever request in flight finishes first
+    (drift_server_wait_any; the wait is recorded, the request's own latency
+    runs from its submission).  A request whose trajectory exceeds cap_bytes
+    returns its final states only (its integration, dense output included, is
+    unchanged; the samples are not stored)."""
     inflight, lat, waits, capped, acc = [], [], [], 0, 0
-    held = deque()  # (request, arrival time): waiting for a slot
-    t_begin = time.perf_counter()
 
-    def submit(r, slot):
-        n, nt = len(r["y0"]), r["nt"]
-        h = srv.submit(r["method"], r["pot"], r["y0"], ts=np.linspace(0.0, r["t_end"], nt), rtol=r["rtol"],
-                       atol=r["rtol"], precision=precision, want_out=slot is not None,
-                       out=slots.view(slot, nt, n) if slot is not None else None)
-        inflight.append((h, slot))
-
-    def retire(timeout: float) -> bool:
-        """Retire the first request in flight to finish, waiting at most
-        `timeout` s (0: until one does); False when none finished."""
+    def retire():
         nonlocal acc
-        if not inflight:
-            return False
-        handles = [h for h, _ in inflight]
-        if timeout > 0:
-            got = srv.poll_any(handles, timeout)
-            if got is None:
-                return False
-            i, res = got
-        else:
-            i, res = srv.wait_any(handles, timeout=3600.0)
+        i, res = srv.wait_any([h for h, _ in inflight], timeout=3600.0)
         _, slot = inflight.pop(i)
         lat.append(res["latency_s"])
         acc += int(res["accepted"].astype(np.int64).sum())
         if slot is not None:
-            if held:  # the freed slot goes to the oldest request waiting for one
-                r, t_arrival = held.popleft()
-                waits.append(time.perf_counter() - t_arrival)
-                submit(r, slot)
-            else:
-                slots.free.append(slot)
-        return True
+            slots.free.append(slot)
 
+    t_begin = time.perf_counter()
     for r in reqs:
-        if open_loop:  # retire finished requests until this one arrives
-            while True:
-                delay = r["at"] - (time.perf_counter() - t_begin)
-                if delay <= 0:
-                    break
-                if not retire(min(delay, 2e-3)) and not inflight:
-                    time.sleep(min(delay, 2e-3))
+        if open_loop:
+            delay = r["at"] - (time.perf_counter() - t_begin)
+            if delay > 0:
+                time.sleep(delay)
         n, nt = len(r["y0"]), r["nt"]
-        if nt * n * 48 > cap_bytes:
-            capped += 1
-            submit(r, None)
-        elif slots.free and not held:
-            waits.append(0.0)
-            submit(r, slots.free.pop())
-        else:
-            held.append((r, time.perf_counter()))
+        want = nt * n * 48 <= cap_bytes
+        capped += not want
+        slot = None
+        if want:
+            t_want = time.perf_counter()
+            while not slots.free:
+                retire()
+            waits.append(time.perf_counter() - t_want)
+            slot = slots.free.pop()
+        h = srv.submit(r["method"], r["pot"], r["y0"], ts=np.linspace(0.0, r["t_end"], nt), rtol=r["rtol"],
+                       atol=r["rtol"], precision=precision, want_out=want,
+                       out=slots.view(slot, nt, n) if want else None)
+        inflight.append((h, slot))
     while inflight:
-        retire(0.0)
+        retire()
     return time.perf_counter() - t_begin, acc, lat, capped, waits
 
 
